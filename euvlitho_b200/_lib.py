@@ -1,0 +1,157 @@
+"""ctypes binding of libeuvl_b200.so (the C ABI declared in include/euvl_b200.h).
+
+The library is built in-tree by ``euvlitho_b200.build``.  There is no fallback:
+if the shared library is missing or fails to load, every entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libeuvl_b200.so")
+
+EUV_OK = 0
+EUV_ERR_BAD_ARG = 1
+EUV_ERR_CUDA = 2
+EUV_ERR_WORKSPACE = 3
+EUV_ERR_SINGULAR = 4
+EUV_MAX_SLICES = 32
+EUV_PREC_FP64 = 0
+EUV_PREC_MIXED = 1
+
+# Every symbol include/euvl_b200.h declares.
+EXPORTS = (
+    "euv_version", "euv_last_error",
+    "euv_mask_spectrum_workspace_bytes", "euv_mask_spectrum",
+    "euv_amp_workspace_bytes", "euv_amp",
+    "euv_abbe", "euv_m3d_fit",
+    "euv_zgemm", "euv_lu_workspace_bytes", "euv_lu_factor", "euv_lu_solve",
+    "euv_matfun_workspace_bytes", "euv_matfun_cs",
+)
+
+
+class EuvError(RuntimeError):
+    """A C-ABI call returned a non-zero status."""
+
+    def __init__(self, fn: str, code: int, msg: str):
+        super().__init__("%s failed (status %d): %s" % (fn, code, msg))
+        self.code = code
+
+
+class c64(C.Structure):
+    _fields_ = [("re", C.c_double), ("im", C.c_double)]
+
+    @classmethod
+    def of(cls, z) -> "c64":
+        z = complex(z)
+        return cls(z.real, z.imag)
+
+
+class Stack(C.Structure):
+    _fields_ = [
+        ("eps_mo", c64), ("eps_si", c64), ("eps_ru", c64), ("eps_mosi2", c64),
+        ("eps_rusi", c64), ("eps_sio2", c64),
+        ("d_mo", C.c_double), ("d_mosi", C.c_double), ("d_si", C.c_double),
+        ("d_simo", C.c_double), ("d_siru", C.c_double), ("d_ru", C.c_double),
+        ("nml", C.c_int),
+    ]
+
+
+P = C.c_void_p
+
+
+class AmpDesc(C.Structure):
+    _fields_ = [
+        ("n_orders", C.c_int), ("lmax", C.c_int), ("mmax", C.c_int),
+        ("d_lindex", P), ("d_mindex", P),
+        ("dx", C.c_double), ("dy", C.c_double), ("k", C.c_double),
+        ("n_slices", C.c_int),
+        ("eabs", c64 * EUV_MAX_SLICES), ("dabs", C.c_double * EUV_MAX_SLICES),
+        ("refresh_sigma", C.c_int),
+        ("stack", Stack),
+        ("n_units", C.c_int),
+        ("d_kx0", P), ("d_ky0", P), ("d_polar", P), ("d_spec", P),
+        ("n_src", C.c_int), ("d_src_order", P), ("d_src_2kz", P),
+        ("precision", C.c_int), ("m_max", C.c_int),
+    ]
+
+
+class AbbeDesc(C.Structure):
+    _fields_ = [
+        ("xdiv", C.c_int), ("ydiv", C.c_int), ("lpx", C.c_int), ("lpy", C.c_int),
+        ("ncut", C.c_int), ("n_units", C.c_int), ("n_src", C.c_int), ("n_order", C.c_int),
+        ("d_coef", P), ("d_nidx", P), ("d_px", P), ("d_py", P), ("d_row_start", P),
+        ("d_tab_of_unit", P), ("d_img_of_unit", P), ("d_nsrc_of_unit", P),
+        ("n_images", C.c_int), ("d_inv_weight", P),
+    ]
+
+
+class M3dDesc(C.Structure):
+    _fields_ = [
+        ("n_clips", C.c_int), ("n_src", C.c_int), ("ninput", C.c_int), ("n_order", C.c_int),
+        ("n_order_narrow", C.c_int), ("lpx", C.c_int), ("lpy", C.c_int),
+        ("k", C.c_double), ("dx", C.c_double), ("dy", C.c_double), ("z0", C.c_double),
+        ("kx0", C.c_double), ("ky0", C.c_double),
+        ("s_center", C.c_int),
+        ("d_src_l", P), ("d_src_m", P), ("d_src_nidx_narrow", P),
+        ("d_ax_vc", P), ("d_ax_ab", P),
+        ("d_lin", P), ("d_min", P), ("d_xin", P), ("d_pair_order", P),
+    ]
+
+
+_lib: Optional[C.CDLL] = None
+
+
+def _declare(lib: C.CDLL) -> None:
+    i, d, sz, ll = C.c_int, C.c_double, C.c_size_t, C.c_longlong
+    lib.euv_version.restype = C.c_char_p
+    lib.euv_last_error.restype = C.c_char_p
+    lib.euv_mask_spectrum_workspace_bytes.restype = sz
+    lib.euv_mask_spectrum_workspace_bytes.argtypes = [i] * 7
+    lib.euv_mask_spectrum.restype = i
+    lib.euv_mask_spectrum.argtypes = [P, i, i, i, i, i, i, i, i, i, P, P, sz, P]
+    lib.euv_amp_workspace_bytes.restype = sz
+    lib.euv_amp_workspace_bytes.argtypes = [C.POINTER(AmpDesc)]
+    lib.euv_amp.restype = i
+    lib.euv_amp.argtypes = [C.POINTER(AmpDesc), P, P, P, sz, P]
+    lib.euv_abbe.restype = i
+    lib.euv_abbe.argtypes = [C.POINTER(AbbeDesc), P, P, P]
+    lib.euv_m3d_fit.restype = i
+    lib.euv_m3d_fit.argtypes = [C.POINTER(M3dDesc), P, P, P, P, P, P]
+    lib.euv_zgemm.restype = i
+    lib.euv_zgemm.argtypes = [i, i, i, c64, P, P, i, ll, P, i, ll, c64, P, i, ll, c64, i, P, i, P]
+    lib.euv_lu_workspace_bytes.restype = sz
+    lib.euv_lu_workspace_bytes.argtypes = [i, i]
+    lib.euv_lu_factor.restype = i
+    lib.euv_lu_factor.argtypes = [i, P, i, ll, P, P, i, P]
+    lib.euv_lu_solve.restype = i
+    lib.euv_lu_solve.argtypes = [i, i, P, i, ll, P, P, i, ll, i, P]
+    lib.euv_matfun_workspace_bytes.restype = sz
+    lib.euv_matfun_workspace_bytes.argtypes = [i, i]
+    lib.euv_matfun_cs.restype = i
+    lib.euv_matfun_cs.argtypes = [i, P, P, P, P, i, i, i, P, sz, P]
+
+
+def lib() -> C.CDLL:
+    """Load the shared library (raises if it is missing: there is no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                "libeuvl_b200.so not found at %s; build it with `python -m euvlitho_b200.build`"
+                % LIB_PATH)
+        l = C.CDLL(LIB_PATH)
+        _declare(l)
+        _lib = l
+    return _lib
+
+
+def check(fn: str, rc: int) -> None:
+    if rc != EUV_OK:
+        raise EuvError(fn, rc, lib().euv_last_error().decode(errors="replace"))
+
+
+def call(fn: str, *args) -> None:
+    check(fn, getattr(lib(), fn)(*args))

@@ -1,0 +1,54 @@
+"""Drop-in replacements of the reference executables.
+
+  python -m euvlitho_b200.cli intensity   # int.out: ./mask.bin -> emint.csv
+  python -m euvlitho_b200.cli m3d         # m3d.out: ./mask.bin -> inputxx.csv, inputlm.csv
+
+Both run the reference configuration (intensity.cpp:44-91, m3d.cpp:34-95) on
+the GPU; --preset picks another workload.
+"""
+from __future__ import annotations
+
+import argparse
+import sys
+import time
+
+import numpy as np
+import torch
+
+from . import io
+from .config import preset
+from .engine import Plan
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("what", choices=["intensity", "m3d"])
+    ap.add_argument("--preset", default="reference")
+    ap.add_argument("--mask", default="./mask.bin")
+    ap.add_argument("--count", type=int, default=1, help="masks in the file (m3d ndata)")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--pol", default="X", choices=["X", "Y"])
+    a = ap.parse_args(argv)
+    cfg = preset(a.preset)
+    t0 = time.time()
+    plan = Plan(cfg, precision=a.precision, pols=(a.pol,))
+    masks = torch.from_numpy(io.read_mask_bin(a.mask, cfg.ndivx, cfg.ndivy, a.count))
+    if a.what == "intensity":
+        img = plan.intensity(masks[:1]).cpu().numpy()
+        io.write_emint("emint.csv" if a.pol == "X" else "emintY.csv", img[0, 0])
+    else:
+        res = plan.m3d(masks)
+        io.write_inputlm("inputlm.csv", plan.linput, plan.minput, plan.xinput)
+        with open("inputxx.csv", "w"):
+            pass
+        for c in range(masks.shape[0]):
+            a0 = res["a0"][c].cpu().numpy()
+            ax = res["ax"][c].cpu().numpy()
+            ay = res["ay"][c].cpu().numpy()
+            io.write_inputxx("inputxx.csv" if c == 0 else "inputxx_%d.csv" % c, a0, ax, ay, plan.xinput)
+    print("elapsed time (s) %.3f" % (time.time() - t0))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

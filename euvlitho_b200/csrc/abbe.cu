@@ -1,0 +1,194 @@
+// Fused Abbe imaging (replaces intensity.cpp:248-408).
+//
+// The reference, per source point: builds the E field of every pupil order on
+// the host (rotate(), pupil phase, defocus), scatters it into three XDIV^2
+// grids, copies each to the GPU, runs a cuFFT Z2Z inverse, copies back and
+// accumulates |Ex|^2+|Ey|^2+|Ez|^2.  Here one kernel does all of it on chip:
+// a CTA owns a stripe of AB_YS image rows (all x) of one unit and loops over
+// that unit's sources:
+//   1. E_c(i) = coef_c(s,i) * Ax(s, nidx(s,i)) for the pupil points (smem);
+//   2. separable inverse DFT, stage y: G_c(l,y) = sum_m E_c(l,m) e^{2 pi i m y/YDIV}
+//      for the stripe (pupil points are stored l-major, so row l is a range);
+//   3. stage x: f_c(x,y) = sum_l G_c(l,y) e^{2 pi i l x/XDIV}, with the twiddle
+//      advanced by a recurrence from an exact start, and |f|^2 accumulated in
+//      registers.
+// Only the DFT of the non-zero pupil box is evaluated (the reference FFTs the
+// whole zero-padded grid).  Partial images are added with FP64 atomics.
+#include "common.cuh"
+
+namespace euv {
+
+constexpr int AB_YS = 4;
+constexpr int AB_THREADS = 256;
+constexpr int AB_XPT = 4;  // x values per thread: xdiv <= 1024
+
+struct AbbeParams {
+  int xdiv, ydiv, lpx, lpy, bx, by, ncut, n_src, n_order, nsplit;
+  const double2* coef;
+  const int* nidx;
+  const int* py;
+  const int* row_start;
+  const int* tab_of_unit;
+  const int* img_of_unit;
+  const int* nsrc_of_unit;
+  const double* inv_weight;
+};
+
+__global__ void __launch_bounds__(AB_THREADS) abbe_kernel(AbbeParams p, const double2* ax,
+                                                          double* image) {
+  extern __shared__ double2 sm[];
+  double2* E = sm;                                   // [ncut][3]
+  double2* G = E + (size_t)p.ncut * 3;                // [YS][bx][3]
+  double2* twy = G + (size_t)AB_YS * p.bx * 3;        // [YS][by]
+  const int u = blockIdx.z;
+  const int y0 = blockIdx.x * AB_YS;
+  const int tid = threadIdx.x;
+  const int nsrc_u = p.nsrc_of_unit[u];
+  const int img = p.img_of_unit[u];
+  const int ny = (p.ydiv - y0) < AB_YS ? (p.ydiv - y0) : AB_YS;
+
+  for (int idx = tid; idx < AB_YS * p.by; idx += AB_THREADS) {
+    int yy = idx / p.by, mm = idx % p.by;
+    long long q = ((long long)(mm - p.lpy) * (y0 + yy)) % p.ydiv;
+    if (q < 0) q += p.ydiv;
+    double s, c;
+    sincospi(2.0 * (double)q / (double)p.ydiv, &s, &c);
+    twy[idx] = make_double2(c, s);
+  }
+
+  double acc[AB_XPT][AB_YS];
+#pragma unroll
+  for (int a = 0; a < AB_XPT; ++a)
+#pragma unroll
+    for (int b = 0; b < AB_YS; ++b) acc[a][b] = 0.0;
+
+  for (int s = blockIdx.y; s < nsrc_u; s += p.nsplit) {
+    __syncthreads();
+    const long long base = ((long long)p.tab_of_unit[u] * p.n_src + s);
+    const double2* axs = ax + ((long long)u * p.n_src + s) * p.n_order;
+    for (int i = tid; i < p.ncut; i += AB_THREADS) {
+      const int n = p.nidx[base * p.ncut + i];
+      cplx e0 = mk(0, 0), e1 = mk(0, 0), e2 = mk(0, 0);
+      if (n >= 0) {
+        double2 a2 = axs[n];
+        cplx a = mk(a2.x, a2.y);
+        const double2* cf = p.coef + (base * p.ncut + i) * 3;
+        e0 = mk(cf[0].x, cf[0].y) * a;
+        e1 = mk(cf[1].x, cf[1].y) * a;
+        e2 = mk(cf[2].x, cf[2].y) * a;
+      }
+      E[i * 3 + 0] = make_double2(e0.x, e0.y);
+      E[i * 3 + 1] = make_double2(e1.x, e1.y);
+      E[i * 3 + 2] = make_double2(e2.x, e2.y);
+    }
+    __syncthreads();
+    // stage y
+    for (int o = tid; o < AB_YS * p.bx * 3; o += AB_THREADS) {
+      const int c = o % 3, lx = (o / 3) % p.bx, yy = o / (3 * p.bx);
+      cplx g = mk(0, 0);
+      const int i0 = p.row_start[lx], i1 = p.row_start[lx + 1];
+      for (int i = i0; i < i1; ++i) {
+        double2 e = E[i * 3 + c];
+        double2 t = twy[yy * p.by + (p.py[i] + p.lpy)];
+        g = g + mk(e.x, e.y) * mk(t.x, t.y);
+      }
+      G[o] = make_double2(g.x, g.y);
+    }
+    __syncthreads();
+    // stage x + |f|^2
+#pragma unroll
+    for (int a = 0; a < AB_XPT; ++a) {
+      const int x = tid + a * AB_THREADS;
+      if (x < p.xdiv) {
+        long long q0 = ((long long)(-p.lpx) * x) % p.xdiv;
+        if (q0 < 0) q0 += p.xdiv;
+        double s0, c0, s1, c1;
+        sincospi(2.0 * (double)q0 / (double)p.xdiv, &s0, &c0);
+        sincospi(2.0 * (double)x / (double)p.xdiv, &s1, &c1);
+        cplx w = mk(c0, s0);
+        const cplx r = mk(c1, s1);
+        cplx f[AB_YS][3];
+#pragma unroll
+        for (int b = 0; b < AB_YS; ++b) f[b][0] = f[b][1] = f[b][2] = mk(0, 0);
+        for (int lx = 0; lx < p.bx; ++lx) {
+#pragma unroll
+          for (int b = 0; b < AB_YS; ++b) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+              double2 g = G[(b * p.bx + lx) * 3 + c];
+              f[b][c] = f[b][c] + mk(g.x, g.y) * w;
+            }
+          }
+          w = w * r;
+        }
+#pragma unroll
+        for (int b = 0; b < AB_YS; ++b)
+          acc[a][b] += f[b][0].x * f[b][0].x + f[b][0].y * f[b][0].y + f[b][1].x * f[b][1].x +
+                       f[b][1].y * f[b][1].y + f[b][2].x * f[b][2].x + f[b][2].y * f[b][2].y;
+      }
+    }
+  }
+  const double wgt = p.inv_weight[img];
+  double* im = image + (size_t)img * p.xdiv * p.ydiv;
+#pragma unroll
+  for (int a = 0; a < AB_XPT; ++a) {
+    const int x = tid + a * AB_THREADS;
+    if (x < p.xdiv)
+#pragma unroll
+      for (int b = 0; b < AB_YS; ++b)
+        if (b < ny) atomicAdd(&im[(size_t)x * p.ydiv + y0 + b], acc[a][b] * wgt);
+  }
+}
+
+}  // namespace euv
+
+using namespace euv;
+
+extern "C" int euv_abbe(const euv_abbe_desc* d, const euv_c64* d_ax, double* d_image,
+                        void* stream_) {
+  if (!d || !d_ax || !d_image || d->xdiv <= 0 || d->ydiv <= 0 ||
+      d->xdiv > AB_THREADS * AB_XPT || d->lpx < 0 || d->lpy < 0 || d->ncut <= 0 ||
+      d->n_units <= 0 || d->n_src <= 0 || d->n_order <= 0 || !d->d_coef || !d->d_nidx ||
+      !d->d_px || !d->d_py || !d->d_row_start || !d->d_tab_of_unit || !d->d_img_of_unit || !d->d_nsrc_of_unit || !d->d_inv_weight ||
+      d->n_images <= 0 || d->n_units > 65535) {
+    euv_set_error("euv_abbe: bad arguments");
+    return EUV_ERR_BAD_ARG;
+  }
+  cudaStream_t stream = (cudaStream_t)stream_;
+  AbbeParams p;
+  p.xdiv = d->xdiv;
+  p.ydiv = d->ydiv;
+  p.lpx = d->lpx;
+  p.lpy = d->lpy;
+  p.bx = 2 * d->lpx + 1;
+  p.by = 2 * d->lpy + 1;
+  p.ncut = d->ncut;
+  p.n_src = d->n_src;
+  p.n_order = d->n_order;
+  p.coef = reinterpret_cast<const double2*>(d->d_coef);
+  p.nidx = d->d_nidx;
+  p.py = d->d_py;
+  p.row_start = d->d_row_start;
+  p.tab_of_unit = d->d_tab_of_unit;
+  p.img_of_unit = d->d_img_of_unit;
+  p.nsrc_of_unit = d->d_nsrc_of_unit;
+  p.inv_weight = d->d_inv_weight;
+  const int ystripes = (d->ydiv + AB_YS - 1) / AB_YS;
+  int nsplit = (2 * 148 + ystripes * d->n_units - 1) / (ystripes * d->n_units);
+  if (nsplit < 1) nsplit = 1;
+  if (nsplit > d->n_src) nsplit = d->n_src;
+  p.nsplit = nsplit;
+  size_t smem = ((size_t)d->ncut * 3 + (size_t)AB_YS * p.bx * 3 + (size_t)AB_YS * p.by) *
+                sizeof(double2);
+  if (smem > 227 * 1024) {
+    euv_set_error("euv_abbe: pupil too large for one CTA (%zu bytes of shared memory)", smem);
+    return EUV_ERR_BAD_ARG;
+  }
+  EUV_CUDA_TRY(cudaFuncSetAttribute(abbe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem));
+  dim3 grid(ystripes, nsplit, d->n_units);
+  abbe_kernel<<<grid, AB_THREADS, smem, stream>>>(p, reinterpret_cast<const double2*>(d_ax),
+                                                  d_image);
+  EUV_LAUNCH_CHECK();
+  return EUV_OK;
+}

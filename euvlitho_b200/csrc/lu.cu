@@ -1,0 +1,286 @@
+// Batched complex FP64 LU with partial pivoting and triangular solves.
+//
+// Replaces matinv (header.h:1468-1557: Eigen colPivHouseholderQr for N<=5000,
+// cuSOLVER Xgetrf/Xgetrs with host round trips above).  The reference only ever
+// applies an inverse to a matrix, so the library factors once and solves with
+// the right-hand sides it needs.
+//
+// Blocked right-looking LU, panel width LU_NB:
+//   panel  : one CTA per matrix factors columns [j0, j0+nb) of rows [j0, n)
+//            (pivot = first max of |re|+|im| as LAPACK izamax, row swap inside
+//            the panel, scale, rank-1 update), in global memory (L2 resident);
+//   laswp  : the panel's row swaps applied to the other columns;
+//   trsm   : U12 = L11^-1 A12 (unit lower, L11 staged in shared memory);
+//   update : A22 -= L21 U12 with the batched DMMA zgemm.
+#include "common.cuh"
+
+namespace euv {
+
+int zgemm(int m, int n, int k, cplx alpha, const double* scale, const double2* a, long long lda,
+          long long sa, const double2* b, long long ldb, long long sb, cplx beta, double2* c,
+          long long ldc, long long sc, cplx diag, int batch, const int* steps, int step,
+          cudaStream_t stream);
+
+constexpr int LU_NB = 32;
+constexpr int LU_PANEL_THREADS = 512;
+
+__device__ __forceinline__ cplx ld2(const double2* p) {
+  double2 v = *p;
+  return mk(v.x, v.y);
+}
+__device__ __forceinline__ void st2(double2* p, cplx v) { *p = make_double2(v.x, v.y); }
+
+__global__ void __launch_bounds__(LU_PANEL_THREADS) lu_panel_kernel(int n, int j0, int jb,
+                                                                    double2* A, long long lda,
+                                                                    long long sa, int* ipiv,
+                                                                    int* info) {
+  A += (long long)blockIdx.x * sa;
+  ipiv += (long long)blockIdx.x * n;
+  __shared__ double red_v[LU_PANEL_THREADS / 32];
+  __shared__ int red_i[LU_PANEL_THREADS / 32];
+  __shared__ int s_piv;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nthr = blockDim.x;
+  for (int jj = j0; jj < j0 + jb; ++jj) {
+    // pivot search: first index of max |re|+|im| in rows jj..n-1
+    double best = -1.0;
+    int bidx = n;
+    for (int r = jj + tid; r < n; r += nthr) {
+      double v = cabs1(ld2(&A[r + (long long)jj * lda]));
+      if (v > best) {
+        best = v;
+        bidx = r;
+      }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      double ov = __shfl_down_sync(0xffffffffu, best, off);
+      int oi = __shfl_down_sync(0xffffffffu, bidx, off);
+      if (ov > best || (ov == best && oi < bidx)) {
+        best = ov;
+        bidx = oi;
+      }
+    }
+    if (lane == 0) {
+      red_v[warp] = best;
+      red_i[warp] = bidx;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      double bv = red_v[0];
+      int bi = red_i[0];
+      for (int w = 1; w < nthr / 32; ++w) {
+        if (red_v[w] > bv || (red_v[w] == bv && red_i[w] < bi)) {
+          bv = red_v[w];
+          bi = red_i[w];
+        }
+      }
+      if (bi >= n) bi = jj;
+      s_piv = bi;
+      ipiv[jj] = bi;
+    }
+    __syncthreads();
+    const int piv = s_piv;
+    if (piv != jj) {
+      for (int c = j0 + tid; c < j0 + jb; c += nthr) {
+        double2 t = A[jj + (long long)c * lda];
+        A[jj + (long long)c * lda] = A[piv + (long long)c * lda];
+        A[piv + (long long)c * lda] = t;
+      }
+    }
+    __syncthreads();
+    const cplx d = ld2(&A[jj + (long long)jj * lda]);
+    if (d.x == 0.0 && d.y == 0.0) {
+      if (tid == 0 && info[blockIdx.x] == 0) info[blockIdx.x] = jj + 1;
+      __syncthreads();
+      continue;
+    }
+    const cplx inv = cdiv(mk(1.0, 0.0), d);
+    for (int r = jj + 1 + tid; r < n; r += nthr) {
+      double2* p = &A[r + (long long)jj * lda];
+      st2(p, ld2(p) * inv);
+    }
+    __syncthreads();
+    const int rows = n - jj - 1;
+    const int cols = j0 + jb - jj - 1;
+    if (rows > 0 && cols > 0) {
+      for (int idx = tid; idx < rows * cols; idx += nthr) {
+        int r = jj + 1 + idx % rows;
+        int c = jj + 1 + idx / rows;
+        double2* p = &A[r + (long long)c * lda];
+        st2(p, ld2(p) - ld2(&A[r + (long long)jj * lda]) * ld2(&A[jj + (long long)c * lda]));
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Row swaps ipiv[j0..j0+jb) applied to every column outside [skip0, skip1).
+__global__ void lu_laswp_kernel(int n, int ncols, int j0, int jb, int skip0, int skip1,
+                                double2* A, long long lda, long long sa, const int* ipiv,
+                                long long ipiv_stride) {
+  const int b = blockIdx.y;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncols || (c >= skip0 && c < skip1)) return;
+  A += (long long)b * sa;
+  ipiv += (long long)b * ipiv_stride;
+  for (int jj = j0; jj < j0 + jb; ++jj) {
+    int p = ipiv[jj];
+    if (p != jj) {
+      double2 t = A[jj + (long long)c * lda];
+      A[jj + (long long)c * lda] = A[p + (long long)c * lda];
+      A[p + (long long)c * lda] = t;
+    }
+  }
+}
+
+// X = T^-1 X for a jb x jb triangular block T of the factor (unit lower when
+// lower != 0, non-unit upper otherwise) and the jb-row slab X of `ncols`
+// columns.  One thread per column; T staged in shared memory.
+__global__ void lu_trsm_block_kernel(int jb, int ncols, int lower, const double2* T,
+                                     long long ldt, long long st, double2* X, long long ldx,
+                                     long long sx) {
+  __shared__ double2 Ts[LU_NB][LU_NB + 1];
+  const int b = blockIdx.y;
+  T += (long long)b * st;
+  X += (long long)b * sx;
+  for (int idx = threadIdx.x; idx < jb * jb; idx += blockDim.x) {
+    int r = idx % jb, c = idx / jb;
+    Ts[r][c] = T[r + (long long)c * ldt];
+  }
+  __syncthreads();
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= ncols) return;
+  cplx x[LU_NB];
+#pragma unroll
+  for (int r = 0; r < LU_NB; ++r)
+    if (r < jb) x[r] = ld2(&X[r + (long long)col * ldx]);
+  if (lower) {
+#pragma unroll
+    for (int r = 0; r < LU_NB; ++r) {
+      if (r < jb) {
+        cplx s = x[r];
+#pragma unroll
+        for (int q = 0; q < LU_NB; ++q)
+          if (q < r) s = s - mk(Ts[r][q].x, Ts[r][q].y) * x[q];
+        x[r] = s;
+      }
+    }
+  } else {
+#pragma unroll
+    for (int r = LU_NB - 1; r >= 0; --r) {
+      if (r < jb) {
+        cplx s = x[r];
+#pragma unroll
+        for (int q = 0; q < LU_NB; ++q)
+          if (q > r && q < jb) s = s - mk(Ts[r][q].x, Ts[r][q].y) * x[q];
+        x[r] = cdiv(s, mk(Ts[r][r].x, Ts[r][r].y));
+      }
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < LU_NB; ++r)
+    if (r < jb) st2(&X[r + (long long)col * ldx], x[r]);
+}
+
+__global__ void zero_int_kernel(int* p, int n) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = 0;
+}
+
+int lu_factor(int n, double2* A, long long lda, long long sa, int* ipiv, int* info, int batch,
+              cudaStream_t stream) {
+  if (n <= 0 || batch <= 0) return EUV_OK;
+  zero_int_kernel<<<(batch + 255) / 256, 256, 0, stream>>>(info, batch);
+  EUV_LAUNCH_CHECK();
+  for (int j0 = 0; j0 < n; j0 += LU_NB) {
+    const int jb = (n - j0) < LU_NB ? (n - j0) : LU_NB;
+    lu_panel_kernel<<<batch, LU_PANEL_THREADS, 0, stream>>>(n, j0, jb, A, lda, sa, ipiv, info);
+    EUV_LAUNCH_CHECK();
+    dim3 gs((n + 127) / 128, batch);
+    lu_laswp_kernel<<<gs, 128, 0, stream>>>(n, n, j0, jb, j0, j0 + jb, A, lda, sa, ipiv, n);
+    EUV_LAUNCH_CHECK();
+    const int rest = n - j0 - jb;
+    if (rest > 0) {
+      dim3 gt((rest + 127) / 128, batch);
+      lu_trsm_block_kernel<<<gt, 128, 0, stream>>>(jb, rest, 1, A + j0 + (long long)j0 * lda,
+                                                    lda, sa, A + j0 + (long long)(j0 + jb) * lda,
+                                                    lda, sa);
+      EUV_LAUNCH_CHECK();
+      int rc = zgemm(rest, rest, jb, mk(-1.0, 0.0), nullptr, A + (j0 + jb) + (long long)j0 * lda,
+                     lda, sa, A + j0 + (long long)(j0 + jb) * lda, lda, sa, mk(1.0, 0.0),
+                     A + (j0 + jb) + (long long)(j0 + jb) * lda, lda, sa, mk(0.0, 0.0), batch,
+                     nullptr, 0, stream);
+      if (rc != EUV_OK) return rc;
+    }
+  }
+  return EUV_OK;
+}
+
+int lu_solve(int n, int nrhs, const double2* LU, long long lda, long long sa, const int* ipiv,
+             double2* B, long long ldb, long long sb, int batch, cudaStream_t stream) {
+  if (n <= 0 || nrhs <= 0 || batch <= 0) return EUV_OK;
+  dim3 gs((nrhs + 127) / 128, batch);
+  lu_laswp_kernel<<<gs, 128, 0, stream>>>(n, nrhs, 0, n, 0, 0, B, ldb, sb, ipiv, n);
+  EUV_LAUNCH_CHECK();
+  // forward: L y = b (unit lower)
+  for (int j0 = 0; j0 < n; j0 += LU_NB) {
+    const int jb = (n - j0) < LU_NB ? (n - j0) : LU_NB;
+    lu_trsm_block_kernel<<<gs, 128, 0, stream>>>(jb, nrhs, 1, LU + j0 + (long long)j0 * lda, lda,
+                                                  sa, B + j0, ldb, sb);
+    EUV_LAUNCH_CHECK();
+    const int rest = n - j0 - jb;
+    if (rest > 0) {
+      int rc = zgemm(rest, nrhs, jb, mk(-1.0, 0.0), nullptr, LU + (j0 + jb) + (long long)j0 * lda,
+                     lda, sa, B + j0, ldb, sb, mk(1.0, 0.0), B + j0 + jb, ldb, sb, mk(0.0, 0.0),
+                     batch, nullptr, 0, stream);
+      if (rc != EUV_OK) return rc;
+    }
+  }
+  // backward: U x = y
+  const int nblk = (n + LU_NB - 1) / LU_NB;
+  for (int bi = nblk - 1; bi >= 0; --bi) {
+    const int j0 = bi * LU_NB;
+    const int jb = (n - j0) < LU_NB ? (n - j0) : LU_NB;
+    lu_trsm_block_kernel<<<gs, 128, 0, stream>>>(jb, nrhs, 0, LU + j0 + (long long)j0 * lda, lda,
+                                                  sa, B + j0, ldb, sb);
+    EUV_LAUNCH_CHECK();
+    if (j0 > 0) {
+      int rc = zgemm(j0, nrhs, jb, mk(-1.0, 0.0), nullptr, LU + (long long)j0 * lda, lda, sa,
+                     B + j0, ldb, sb, mk(1.0, 0.0), B, ldb, sb, mk(0.0, 0.0), batch, nullptr, 0,
+                     stream);
+      if (rc != EUV_OK) return rc;
+    }
+  }
+  return EUV_OK;
+}
+
+}  // namespace euv
+
+extern "C" size_t euv_lu_workspace_bytes(int n, int batch) {
+  (void)n;
+  (void)batch;
+  return 0;
+}
+
+extern "C" int euv_lu_factor(int n, euv_c64* d_a, int lda, long long stride_a, int* d_ipiv,
+                             int* d_info, int batch, void* stream) {
+  if (n < 0 || lda < (n > 0 ? n : 1) || batch < 0 || (n > 0 && batch > 0 && (!d_a || !d_ipiv || !d_info))) {
+    euv_set_error("euv_lu_factor: bad arguments (n=%d lda=%d batch=%d)", n, lda, batch);
+    return EUV_ERR_BAD_ARG;
+  }
+  return euv::lu_factor(n, reinterpret_cast<double2*>(d_a), lda, stride_a, d_ipiv, d_info, batch,
+                        (cudaStream_t)stream);
+}
+
+extern "C" int euv_lu_solve(int n, int nrhs, const euv_c64* d_lu, int lda, long long stride_a,
+                            const int* d_ipiv, euv_c64* d_b, int ldb, long long stride_b,
+                            int batch, void* stream) {
+  if (n < 0 || nrhs < 0 || lda < (n > 0 ? n : 1) || ldb < (n > 0 ? n : 1) || batch < 0) {
+    euv_set_error("euv_lu_solve: bad arguments (n=%d nrhs=%d lda=%d ldb=%d)", n, nrhs, lda, ldb);
+    return EUV_ERR_BAD_ARG;
+  }
+  return euv::lu_solve(n, nrhs, reinterpret_cast<const double2*>(d_lu), lda, stride_a, d_ipiv,
+                       reinterpret_cast<double2*>(d_b), ldb, stride_b, batch,
+                       (cudaStream_t)stream);
+}

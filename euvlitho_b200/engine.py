@@ -1,0 +1,383 @@
+"""Host driver: the loops of intensity.cpp / m3d.cpp over the batched C ABI.
+
+A :class:`Plan` owns, per configuration, the resident device tables (order set,
+pupil set, per-family source lists and Abbe E-field factors, the mask-independent
+vacuum/absorber solves of m3d) and a workspace.  Its methods enqueue work on the
+current torch CUDA stream through ``libeuvl_b200.so``; device buffers are torch
+tensors.  Nothing here computes physics on the host.
+
+Entry points mirror the reference:
+  * :meth:`Plan.amp`        -- ampS (header.h:1208-1466), batched over units;
+  * :meth:`Plan.intensity`  -- the Abbe image of intensity.cpp (emint.csv);
+  * :meth:`Plan.m3d`        -- the M3D parameters of m3d.cpp (inputxx.csv).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+import torch
+
+from . import _lib as L
+from .config import PI, SimConfig
+from . import tables as T
+
+_POL = {"X": 0, "Y": 1}
+
+
+def _ptr(t: Optional[torch.Tensor]) -> Optional[int]:
+    return None if t is None else t.data_ptr()
+
+
+def _stream() -> int:
+    return torch.cuda.current_stream().cuda_stream
+
+
+def stack_struct(cfg: SimConfig) -> L.Stack:
+    s = cfg.stack
+    return L.Stack(L.c64.of(s.n_mo ** 2), L.c64.of(s.n_si ** 2), L.c64.of(s.n_ru ** 2),
+                   L.c64.of(s.n_mosi2 ** 2), L.c64.of(s.n_rusi ** 2), L.c64.of(s.n_sio2 ** 2),
+                   s.d_mo, s.d_mosi, s.d_si, s.d_simo, s.d_siru, s.d_ru, s.nml)
+
+
+@dataclass
+class OrderSet:
+    kind: str
+    lmax: int
+    mmax: int
+    lidx: np.ndarray
+    midx: np.ndarray
+
+    @property
+    def n(self) -> int:
+        return len(self.lidx)
+
+
+class Workspace:
+    """Grow-only device scratch buffer."""
+
+    def __init__(self, device):
+        self.device = device
+        self.buf: Optional[torch.Tensor] = None
+
+    def get(self, nbytes: int) -> torch.Tensor:
+        nbytes = max(int(nbytes), 256)
+        if self.buf is None or self.buf.numel() < nbytes:
+            self.buf = None
+            self.buf = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+        return self.buf
+
+
+class Plan:
+    """Resident tables and workspace for one configuration."""
+
+    def __init__(self, cfg: SimConfig, device: Optional[torch.device] = None,
+                 precision: str = "fp64", pols: Sequence[str] = ("X",)):
+        L.lib()  # fail loudly if the library is missing
+        if not torch.cuda.is_available():
+            raise RuntimeError("euvlitho_b200 needs a CUDA device")
+        self.cfg = cfg
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self.precision = {"fp64": L.EUV_PREC_FP64, "mixed": L.EUV_PREC_MIXED}[precision]
+        self.pols = tuple(pols)
+        for p in self.pols:
+            if p not in _POL:
+                raise ValueError("polarisation must be 'X' or 'Y'")
+        if cfg.nabs > L.EUV_MAX_SLICES:
+            raise ValueError("at most %d absorber slices" % L.EUV_MAX_SLICES)
+        if cfg.fdivx % cfg.ndivx or cfg.fdivy % cfg.ndivy:
+            raise ValueError("the Fourier grid must refine the mask grid by an integer factor")
+        lmax, mmax = cfg.order_limits()
+        li, mi = T.order_set(cfg.order_kind, lmax, mmax)
+        self.orders = OrderSet(cfg.order_kind, lmax, mmax, li, mi)
+        self.pos = T.order_positions(li, mi)
+        kxy_max = (abs(cfg.kx0) + 2 * PI * (lmax + 1) / cfg.dx) ** 2 + \
+                  (abs(cfg.ky0) + 2 * PI * (mmax + 1) / cfg.dy) ** 2
+        if kxy_max >= cfg.k ** 2:
+            # header.h:1283 takes a real square root: the reference gives NaN there
+            raise ValueError("order set reaches evanescent orders (|k_xy| >= k); the reference "
+                             "computes NaN for them; reduce the order cut")
+        self.linput, self.minput, self.xinput, _ = T.pupil_set(cfg)
+        self.ncut = len(self.linput)
+        self.ndivs, self.fams = T.sources(cfg)
+        self.sdivsum = sum(len(f.pts) for f in self.fams)
+        if self.sdivsum == 0:
+            raise ValueError("the illumination has no source point")
+        self.work = Workspace(self.device)
+        dev = self.device
+        self._t_l = torch.tensor(li, dtype=torch.int32, device=dev)
+        self._t_m = torch.tensor(mi, dtype=torch.int32, device=dev)
+        self._abbe_tables = None
+        self._m3d_tables = None
+
+    # ------------------------------------------------------------ helpers
+    def _i32(self, a) -> torch.Tensor:
+        return torch.tensor(np.asarray(a, np.int32), dtype=torch.int32, device=self.device)
+
+    def _f64(self, a) -> torch.Tensor:
+        return torch.tensor(np.asarray(a, np.float64), dtype=torch.float64, device=self.device)
+
+    def _c128(self, a) -> torch.Tensor:
+        return torch.tensor(np.asarray(a, np.complex128), dtype=torch.complex128, device=self.device)
+
+    def mask_bytes(self) -> int:
+        return self.cfg.ndivx * self.cfg.ndivy // 8
+
+    def as_mask_tensor(self, masks) -> torch.Tensor:
+        """uint8 device tensor [clips, slices_or_1, nbytes] of packed mask.bin bits."""
+        nb = self.mask_bytes()
+        if isinstance(masks, (bytes, bytearray)):
+            masks = np.frombuffer(masks, np.uint8)
+        t = torch.as_tensor(masks) if not isinstance(masks, torch.Tensor) else masks
+        if t.dtype != torch.uint8:
+            raise TypeError("masks must be packed uint8 (mask.bin layout)")
+        if t.dim() == 1:
+            t = t.view(1, 1, -1)
+        elif t.dim() == 2:
+            t = t.view(t.shape[0], 1, -1)
+        if t.shape[-1] != nb:
+            raise ValueError("each mask must be %d bytes (ndivx*ndivy/8)" % nb)
+        if t.shape[1] not in (1, self.cfg.nabs):
+            raise ValueError("give one mask per clip or one per absorber slice")
+        return t.to(self.device, non_blocking=True).contiguous()
+
+    # ------------------------------------------------------------ spectra
+    def spectra(self, masks: torch.Tensor, lh: int, mh: int, select_vacuum: int = 0,
+                per_slice: bool = True) -> torch.Tensor:
+        """Indicator spectra [clips, slices, (2lh+1)(2mh+1)] (maskamp, header.h:1147-1206)."""
+        cfg = self.cfg
+        n_clips, n_m, nb = masks.shape
+        flat = masks.reshape(n_clips * n_m, nb)
+        out = torch.empty((n_clips * n_m, (2 * lh + 1) * (2 * mh + 1)), dtype=torch.complex128,
+                          device=self.device)
+        wb = L.lib().euv_mask_spectrum_workspace_bytes(n_clips * n_m, cfg.ndivx, cfg.ndivy,
+                                                      cfg.fdivx, cfg.fdivy, lh, mh)
+        ws = self.work.get(wb)
+        L.call("euv_mask_spectrum", flat.data_ptr(), n_clips * n_m, cfg.ndivx, cfg.ndivy,
+               cfg.fdivx, cfg.fdivy, lh, mh, select_vacuum, cfg.yflip_offset, out.data_ptr(), ws.data_ptr(),
+               ws.numel(), _stream())
+        out = out.view(n_clips, n_m, -1)
+        if per_slice and n_m == 1 and cfg.nabs > 1:
+            out = out.expand(n_clips, cfg.nabs, out.shape[-1]).contiguous()
+        return out
+
+    # ------------------------------------------------------------ ampS
+    def amp_desc(self, orders: OrderSet, t_l, t_m, kx0, ky0, polar, spec_of_unit,
+                 src_order, src_2kz, keep) -> L.AmpDesc:
+        cfg = self.cfg
+        d = L.AmpDesc()
+        d.n_orders = orders.n
+        d.lmax, d.mmax = orders.lmax, orders.mmax
+        d.d_lindex, d.d_mindex = _ptr(t_l), _ptr(t_m)
+        d.dx, d.dy, d.k = cfg.dx, cfg.dy, cfg.k
+        d.n_slices = cfg.nabs
+        for n in range(cfg.nabs):
+            d.eabs[n] = L.c64.of(cfg.eabs[n])
+            d.dabs[n] = float(cfg.dabs[n])
+        d.refresh_sigma = 1 if cfg.refresh_sigma else 0
+        d.stack = stack_struct(cfg)
+        d.n_units = int(kx0.numel())
+        d.d_kx0, d.d_ky0, d.d_polar, d.d_spec = _ptr(kx0), _ptr(ky0), _ptr(polar), _ptr(spec_of_unit)
+        d.n_src = int(src_order.shape[1])
+        d.d_src_order, d.d_src_2kz = _ptr(src_order), _ptr(src_2kz)
+        d.precision = self.precision
+        d.m_max = 0
+        keep.extend([t_l, t_m, kx0, ky0, polar, spec_of_unit, src_order, src_2kz])
+        return d
+
+    def run_amp(self, desc: L.AmpDesc, spectra: torch.Tensor, ax: torch.Tensor) -> None:
+        wb = L.lib().euv_amp_workspace_bytes(C.byref(desc))
+        if wb == 0:
+            raise ValueError("invalid ampS descriptor")
+        ws = self.work.get(wb)
+        L.call("euv_amp", C.byref(desc), spectra.data_ptr(), ax.data_ptr(), ws.data_ptr(),
+               ws.numel(), _stream())
+
+    def src_columns(self, kx0: float, ky0: float, srcs: Sequence[Tuple[int, int]], n_src: int):
+        """Order index and 2 kz of each source column (header.h:1396-1409)."""
+        cfg = self.cfg
+        order = np.full(n_src, -1, np.int32)
+        kz2 = np.zeros(n_src, np.float64)
+        for s, (ls, ms) in enumerate(srcs):
+            kx = kx0 + ls * 2.0 * PI / cfg.dx
+            ky = ky0 + ms * 2.0 * PI / cfg.dy
+            kz2[s] = 2.0 * math.sqrt(cfg.k * cfg.k - kx * kx - ky * ky)
+            order[s] = self.pos.get((ls, ms), -1)
+        return order, kz2
+
+    def amp(self, masks, polar: str = "X", kx0: Optional[float] = None,
+            ky0: Optional[float] = None) -> Tuple[torch.Tensor, List[Tuple[int, int]]]:
+        """ampS for every clip at one incidence: Ax[clip][s][N] for the NA-circle
+        source orders (header.h:1394-1465); returns (Ax, source order list)."""
+        cfg = self.cfg
+        m = self.as_mask_tensor(masks)
+        nc = m.shape[0]
+        kx0 = cfg.kx0 if kx0 is None else kx0
+        ky0 = cfg.ky0 if ky0 is None else ky0
+        srcs = T.na_sources(cfg)
+        o, kz2 = self.src_columns(kx0, ky0, srcs, len(srcs))
+        spec = self.spectra(m, 2 * self.orders.lmax, 2 * self.orders.mmax)
+        keep: list = []
+        desc = self.amp_desc(self.orders, self._t_l, self._t_m, self._f64([kx0] * nc),
+                             self._f64([ky0] * nc), self._i32([_POL[polar]] * nc),
+                             self._i32(range(nc)), self._i32(np.tile(o, (nc, 1))),
+                             self._f64(np.tile(kz2, (nc, 1))), keep)
+        ax = torch.empty((nc, len(srcs), self.orders.n), dtype=torch.complex128, device=self.device)
+        self.run_amp(desc, spec, ax)
+        return ax, srcs
+
+    # ------------------------------------------------------------ Abbe
+    def abbe_tables(self):
+        if self._abbe_tables is not None:
+            return self._abbe_tables
+        cfg = self.cfg
+        n_src = max(len(f.pts) for f in self.fams)
+        coefs, nidxs, kx0s, ky0s, orders, kz2s, pols, nsrcs = [], [], [], [], [], [], [], []
+        for p in self.pols:
+            for f in self.fams:
+                c, n = T.abbe_table(cfg, p, self.ndivs, f, self.pos, self.linput, self.minput, n_src)
+                coefs.append(c)
+                nidxs.append(n)
+                sx0, sy0 = T.family_offsets(cfg, self.ndivs, f)
+                o, kz2 = self.src_columns(sx0, sy0, f.pts, n_src)
+                if np.any(o[: len(f.pts)] < 0):
+                    raise ValueError("a source order of family %s is outside the order set" %
+                                     ((f.nsx, f.nsy),))
+                kx0s.append(sx0)
+                ky0s.append(sy0)
+                orders.append(o)
+                kz2s.append(kz2)
+                pols.append(_POL[p])
+                nsrcs.append(len(f.pts))
+        tb = dict(
+            n_src=n_src,
+            coef=self._c128(np.stack(coefs)),
+            nidx=self._i32(np.stack(nidxs)),
+            px=self._i32(self.linput), py=self._i32(self.minput),
+            row_start=self._i32(T.row_starts(self.linput, cfg.lpmaxX)),
+            kx0=np.array(kx0s), ky0=np.array(ky0s), order=np.stack(orders), kz2=np.stack(kz2s),
+            pol=np.array(pols, np.int32), nsrc=np.array(nsrcs, np.int32),
+        )
+        self._abbe_tables = tb
+        return tb
+
+    def intensity(self, masks, out: Optional[torch.Tensor] = None) -> torch.Tensor:
+        """Abbe images [clips, pols, XDIV, YDIV] (intensity.cpp:219-408); I[x][y]."""
+        cfg = self.cfg
+        m = self.as_mask_tensor(masks)
+        nc = m.shape[0]
+        tb = self.abbe_tables()
+        ntab = len(tb["pol"])
+        spec = self.spectra(m, 2 * self.orders.lmax, 2 * self.orders.mmax)
+        # units: clip-major, then (pol, family) table order
+        U = nc * ntab
+        tab = np.tile(np.arange(ntab, dtype=np.int32), nc)
+        clip = np.repeat(np.arange(nc, dtype=np.int32), ntab)
+        npol = len(self.pols)
+        nf = len(self.fams)
+        img = clip * npol + (tab // nf)
+        keep: list = []
+        desc = self.amp_desc(self.orders, self._t_l, self._t_m, self._f64(tb["kx0"][tab]),
+                             self._f64(tb["ky0"][tab]), self._i32(tb["pol"][tab]),
+                             self._i32(clip), self._i32(tb["order"][tab]),
+                             self._f64(tb["kz2"][tab]), keep)
+        ax = torch.empty((U, tb["n_src"], self.orders.n), dtype=torch.complex128, device=self.device)
+        self.run_amp(desc, spec, ax)
+        if out is None:
+            out = torch.zeros((nc, npol, cfg.xdiv, cfg.ydiv), dtype=torch.float64, device=self.device)
+        else:
+            out.zero_()
+        t_tab, t_img, t_ns = self._i32(tab), self._i32(img), self._i32(tb["nsrc"][tab])
+        inv_w = self._f64([1.0 / self.sdivsum] * (nc * npol))
+        ad = L.AbbeDesc()
+        ad.xdiv, ad.ydiv = cfg.xdiv, cfg.ydiv
+        ad.lpx, ad.lpy = cfg.lpmaxX, cfg.lpmaxY
+        ad.ncut, ad.n_units, ad.n_src, ad.n_order = self.ncut, U, tb["n_src"], self.orders.n
+        ad.d_coef, ad.d_nidx = _ptr(tb["coef"]), _ptr(tb["nidx"])
+        ad.d_px, ad.d_py, ad.d_row_start = _ptr(tb["px"]), _ptr(tb["py"]), _ptr(tb["row_start"])
+        ad.d_tab_of_unit, ad.d_img_of_unit, ad.d_nsrc_of_unit = _ptr(t_tab), _ptr(t_img), _ptr(t_ns)
+        ad.n_images = nc * npol
+        ad.d_inv_weight = _ptr(inv_w)
+        L.call("euv_abbe", C.byref(ad), ax.data_ptr(), out.data_ptr(), _stream())
+        self._last_keep = (keep, t_tab, t_img, t_ns, inv_w, ax)
+        return out
+
+    # ------------------------------------------------------------ M3D
+    def m3d_tables(self):
+        if self._m3d_tables is not None:
+            return self._m3d_tables
+        cfg = self.cfg
+        ln, mn = cfg.order_limits("ellipse", 1.5)  # m3d.cpp:107-129
+        nli, nmi = T.order_set("ellipse", ln, mn)
+        narrow = OrderSet("ellipse", ln, mn, nli, nmi)
+        npos = T.order_positions(nli, nmi)
+        srcs = T.na_sources(cfg)
+        ns = len(srcs)
+        src_nn = np.array([npos.get(s, -1) for s in srcs], np.int32)
+        if np.any(src_nn < 0):
+            raise ValueError("narrow order set misses a source order")
+        pair = np.full((self.ncut, ns), -1, np.int32)
+        for n in range(self.ncut):
+            lp, mp = int(self.linput[n]), int(self.minput[n])
+            for s, (ls, ms) in enumerate(srcs):
+                if T.in_na(cfg, ls + lp, ms + mp):
+                    o = self.pos.get((ls + lp, ms + mp))
+                    if o is None:
+                        raise ValueError("order set misses pupil order %s" % ((ls + lp, ms + mp),))
+                    pair[n, s] = o
+        # mask-independent narrow solves on the all-vacuum / all-absorber masks
+        nb = self.mask_bytes()
+        uni = torch.stack([torch.full((nb,), 255, dtype=torch.uint8),
+                           torch.zeros(nb, dtype=torch.uint8)]).to(self.device)
+        spec = self.spectra(uni.view(2, 1, nb), 2 * ln, 2 * mn)
+        o, kz2 = [], []
+        for (ls, ms) in srcs:
+            kx = cfg.kx0 + ls * 2.0 * PI / cfg.dx
+            ky = cfg.ky0 + ms * 2.0 * PI / cfg.dy
+            kz2.append(2.0 * math.sqrt(cfg.k ** 2 - kx * kx - ky * ky))
+        t_nl, t_nm = self._i32(nli), self._i32(nmi)
+        keep: list = []
+        desc = self.amp_desc(narrow, t_nl, t_nm, self._f64([cfg.kx0] * 2), self._f64([cfg.ky0] * 2),
+                             self._i32([_POL[self.pols[0]]] * 2), self._i32([0, 1]),
+                             self._i32(np.tile(src_nn, (2, 1))), self._f64(np.tile(kz2, (2, 1))), keep)
+        axn = torch.empty((2, ns, narrow.n), dtype=torch.complex128, device=self.device)
+        self.run_amp(desc, spec, axn)
+        tb = dict(
+            narrow=narrow, srcs=srcs, ns=ns,
+            src_l=self._i32([s[0] for s in srcs]), src_m=self._i32([s[1] for s in srcs]),
+            src_nn=self._i32(src_nn), s_center=srcs.index((0, 0)),
+            ax_vc=axn[0].contiguous(), ax_ab=axn[1].contiguous(),
+            lin=self._i32(self.linput), min=self._i32(self.minput), xin=self._i32(self.xinput),
+            pair=self._i32(pair), keep=keep,
+        )
+        self._m3d_tables = tb
+        return tb
+
+    def m3d(self, masks) -> Dict[str, torch.Tensor]:
+        """M3D parameters per clip (m3d.cpp:197-558): 'a0' [clips, ninput] and
+        'ax', 'ay' [clips, ninput] (zero where xinput == 0)."""
+        cfg = self.cfg
+        tb = self.m3d_tables()
+        m = self.as_mask_tensor(masks)
+        ax_wide, srcs = self.amp(m, polar=self.pols[0])
+        fmask = self.spectra(m[:, :1], cfg.lpmaxX, cfg.lpmaxY, select_vacuum=1, per_slice=False)
+        nc = m.shape[0]
+        a0 = torch.empty((nc, self.ncut), dtype=torch.complex128, device=self.device)
+        axp = torch.empty_like(a0)
+        ayp = torch.empty_like(a0)
+        d = L.M3dDesc()
+        d.n_clips, d.n_src, d.ninput, d.n_order = nc, tb["ns"], self.ncut, self.orders.n
+        d.n_order_narrow = tb["narrow"].n
+        d.lpx, d.lpy = cfg.lpmaxX, cfg.lpmaxY
+        d.k, d.dx, d.dy, d.z0, d.kx0, d.ky0 = cfg.k, cfg.dx, cfg.dy, cfg.z0, cfg.kx0, cfg.ky0
+        d.s_center = tb["s_center"]
+        d.d_src_l, d.d_src_m, d.d_src_nidx_narrow = _ptr(tb["src_l"]), _ptr(tb["src_m"]), _ptr(tb["src_nn"])
+        d.d_ax_vc, d.d_ax_ab = _ptr(tb["ax_vc"]), _ptr(tb["ax_ab"])
+        d.d_lin, d.d_min, d.d_xin, d.d_pair_order = _ptr(tb["lin"]), _ptr(tb["min"]), _ptr(tb["xin"]), _ptr(tb["pair"])
+        L.call("euv_m3d_fit", C.byref(d), ax_wide.data_ptr(), fmask.data_ptr(), a0.data_ptr(),
+               axp.data_ptr(), ayp.data_ptr(), _stream())
+        self._last_keep = (ax_wide, fmask)
+        return {"a0": a0, "ax": axp, "ay": ayp, "Ax": ax_wide, "srcs": srcs}

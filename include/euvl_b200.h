@@ -1,0 +1,237 @@
+/*
+ * euvl_b200.h -- C ABI of the B200 EUV mask-3D library (libeuvl_b200.so).
+ *
+ * Drop-in boundary for the rigorous mask-3D solve and Abbe imaging of
+ * takahashi-edalab/EUVlitho.  The reference exposes these as C++ functions in
+ * cnn/include/header.h and the main() loops of cnn/intensity/abbe/intensity.cpp
+ * and cnn/intensity/m3d/m3d.cpp; each entry point below names the reference
+ * code it replaces.
+ *
+ * Conventions
+ *  - Every pointer named d_* is DEVICE memory owned by the caller (e.g. a
+ *    torch tensor); h_* is host memory.  The library allocates nothing on the
+ *    device: scratch space is a caller-provided workspace whose size is given by
+ *    the matching *_workspace_bytes() query.
+ *  - Complex numbers are euv_c64 = {re, im} doubles, layout-compatible with
+ *    cuDoubleComplex, std::complex<double> and torch.complex128.
+ *  - Matrices are column-major (element (i,j) at i + j*ld), batched with an
+ *    element stride between consecutive matrices.
+ *  - `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).
+ *    Work is enqueued asynchronously on it; nothing synchronises the host.
+ *  - Every function returns EUV_OK (0) or an error code; euv_last_error()
+ *    returns a message for the last failure on the calling thread.
+ *  - Thread safety: functions keep no global state besides the per-thread error
+ *    message; concurrent calls on different streams with disjoint buffers are
+ *    safe.
+ */
+#ifndef EUVL_B200_H
+#define EUVL_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EUV_OK 0
+#define EUV_ERR_BAD_ARG 1
+#define EUV_ERR_CUDA 2
+#define EUV_ERR_WORKSPACE 3
+#define EUV_ERR_SINGULAR 4
+
+#define EUV_MAX_SLICES 32
+
+#define EUV_PREC_FP64 0  /* every product in FP64 */
+#define EUV_PREC_MIXED 1 /* bulk products on BF16x3 tensor cores, FP64 solves */
+
+typedef struct {
+  double re, im;
+} euv_c64;
+
+/* Multilayer materials (permittivities) and thicknesses in nm: the constants of
+ * header.h:1217-1230, made parameters. */
+typedef struct {
+  euv_c64 eps_mo, eps_si, eps_ru, eps_mosi2, eps_rusi, eps_sio2;
+  double d_mo, d_mosi, d_si, d_simo, d_siru, d_ru;
+  int nml; /* Mo/Si periods (header.h NML) */
+} euv_stack;
+
+/* Library version and last error. */
+const char* euv_version(void);
+const char* euv_last_error(void);
+
+/* ------------------------------------------------------------------------ */
+/* Mask spectrum: replaces maskamp (header.h:1147-1206) with fourier /
+ * exponential (header.h:1621-1648), and the thin-mask DFT of m3d.cpp:287-327.
+ *
+ * d_bits: n_masks packed masks of ndivx*ndivy bits each, MSB first, bit index
+ *   ndivx*j + i (j = y), exactly the mask.bin layout (intensity.cpp:20-29).
+ * The pattern on the fdivx x fdivy Fourier grid is pixel (i/meshx,
+ * ndivy-1-j/meshy + y_offset) (y flipped, header.h:1159); rows outside the
+ * mask read as absorber.  y_offset = 0 is the shipped header.h; y_offset = 1
+ * reproduces the revision that produced the reference's golden emint.csv /
+ * inputxx.csv (its flip is one row off).  select_vacuum = 0 transforms the
+ * absorber indicator (bit == 0), 1 the vacuum indicator (bit == 1).
+ * d_out[mask][l + (2*lh+1)*m'] = (1/(fdivx*fdivy)) sum_x,y ind(x,y)
+ *   exp(-2 pi i (l x/fdivx + m y/fdivy)),  l in [-lh, lh], m in [-mh, mh].
+ * The permittivity coefficients of header.h:1236-1251 follow as
+ *   eps = 1*delta + (eps_abs - 1) * F,  sigma = delta + (1/eps_abs - 1) * F,
+ *   leps = log(eps_abs) * F (F = absorber-indicator spectrum). */
+size_t euv_mask_spectrum_workspace_bytes(int n_masks, int ndivx, int ndivy, int fdivx, int fdivy,
+                                         int lh, int mh);
+int euv_mask_spectrum(const uint8_t* d_bits, int n_masks, int ndivx, int ndivy, int fdivx,
+                      int fdivy, int lh, int mh, int select_vacuum, int y_offset, euv_c64* d_out,
+                      void* d_work, size_t work_bytes, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Batched ampS: replaces ampS (header.h:1208-1466) with multilayerS
+ * (header.h:5-363), absorberS0 (754-1145), absorberS (365-752), matinv and
+ * matproduct (1468-1619), for n_units independent problems that share one
+ * order set.  A unit is one (clip, Bloch family, polarisation).
+ *
+ * Outputs Ax for the requested source orders:
+ *   d_ax[u][s][n] = Ax[(ls,ms)](n) of header.h:1394-1465, s < n_src, n < N.
+ * Source columns whose order is not in the order set (src_order = -1) get zeros
+ * except that they are never referenced by the callers. */
+typedef struct {
+  int n_orders;          /* Nrange */
+  int lmax, mmax;        /* LMAX, MMAX: spectra cover orders -2LMAX..2LMAX x -2MMAX..2MMAX */
+  const int* d_lindex;   /* [N] */
+  const int* d_mindex;   /* [N] */
+  double dx, dy;         /* clip period (nm) */
+  double k;              /* 2 pi / lambda */
+  int n_slices;          /* NABS; slice 0 = top, n_slices-1 sits on the Ru cap */
+  euv_c64 eabs[EUV_MAX_SLICES];
+  double dabs[EUV_MAX_SLICES];
+  int refresh_sigma;     /* 0: reference behaviour (bottom-slice sigma for all slices) */
+  euv_stack stack;
+  int n_units;
+  const double* d_kx0;   /* [U] incidence kx of the unit's Bloch family (sx0) */
+  const double* d_ky0;   /* [U] */
+  const int* d_polar;    /* [U] 0 = 'X', 1 = 'Y' */
+  const int* d_spec;     /* [U] index c of the unit's clip: slice n spectrum is
+                            d_spectra[(c*n_slices + n) * (4lmax+1)(4mmax+1)] */
+  int n_src;             /* source columns per unit */
+  const int* d_src_order;  /* [U][n_src] order index of each source (-1: none) */
+  const double* d_src_2kz; /* [U][n_src] 2*kz of each source (header.h:1401-1409) */
+  int precision;         /* EUV_PREC_FP64 or EUV_PREC_MIXED */
+  int m_max;             /* upper bound on double-angle steps; <= 0: derived */
+} euv_amp_desc;
+
+size_t euv_amp_workspace_bytes(const euv_amp_desc* desc);
+int euv_amp(const euv_amp_desc* desc, const euv_c64* d_spectra, euv_c64* d_ax, void* d_work,
+            size_t work_bytes, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Fused Abbe imaging: replaces the per-source loop of intensity.cpp:248-408
+ * (E-field through rotate(), pupil phase and defocus, scatter, three cuFFT Z2Z
+ * inverse transforms, |Ex|^2+|Ey|^2+|Ez|^2, sum over sources / SDIVSUM) with one
+ * kernel that keeps the image on chip.
+ *
+ * The config-only factors are precomputed tables (resident per plan):
+ *   d_coef[((t*n_src + s)*ncut + i)*3 + c]  = i k R(c,.) . (polarisation) * phase
+ *                                             / sqrt(k^2 - kx^2)  (or ky)
+ *   d_nidx[(t*n_src + s)*ncut + i]          = order index of pupil point i of
+ *                                             source s (-1: outside the pupil)
+ *   with t = d_tab_of_unit[u] (units of different clips share tables)
+ *   d_px[i], d_py[i]                        = pupil frequency indices (linput, minput)
+ *   d_row_start[l]                          = first pupil point with linput = l - lpx
+ *                                             (points are l-major, as intensity.cpp:166-195
+ *                                             enumerates them; [2*lpx+2] entries)
+ * Image: d_image[img][x*ydiv + y] += (1/weight[img]) * sum over units u with
+ * d_img_of_unit[u] == img, sources s < d_nsrc_of_unit[u], of |f|^2, where f is
+ * the unnormalised inverse DFT of the pupil field (intensity.cpp:369-386). The
+ * image must be zeroed by the caller. */
+typedef struct {
+  int xdiv, ydiv;        /* image grid */
+  int lpx, lpy;          /* pupil box half sizes (lpmaxX, lpmaxY) */
+  int ncut;              /* pupil points */
+  int n_units, n_src, n_order;
+  const euv_c64* d_coef;
+  const int* d_nidx;
+  const int* d_px;
+  const int* d_py;
+  const int* d_row_start;
+  const int* d_tab_of_unit;   /* [U] */
+  const int* d_img_of_unit;   /* [U] */
+  const int* d_nsrc_of_unit;  /* [U] */
+  int n_images;
+  const double* d_inv_weight; /* [n_images] 1/SDIVSUM */
+} euv_abbe_desc;
+
+int euv_abbe(const euv_abbe_desc* desc, const euv_c64* d_ax, double* d_image, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* M3D parameters: replaces m3d.cpp:240-467 (specular vacuum/absorber
+ * amplitudes, thin-mask amplitudes, phase normalisation by the vacuum specular
+ * phase, difference dampxx, 3x3 Cramer least squares a0 + ax*ls + ay*ms per
+ * pupil order).
+ *   d_ax_wide[c][s][n]: rigorous amplitudes of clip c for the NA-circle source
+ *     orders s (enumeration of header.h:1394-1397), n < n_order;
+ *   d_ax_vc / d_ax_ab [s][n']: the same for the all-vacuum / all-absorber mask
+ *     on the narrow order set (m3d.cpp:214-238), n' < n_order_narrow;
+ *   d_src_nidx_narrow[s]: order index of source s in the narrow set;
+ *   s_center: index of source order (0,0);
+ *   d_fmask[c][ip + (2lpx+1)*jp]: vacuum-indicator spectrum (euv_mask_spectrum
+ *     with select_vacuum=1, lh=lpx, mh=lpy);
+ *   d_lin/d_min/d_xin[n]: pupil orders and the xinput flag (m3d.cpp:160-195);
+ *   d_pair_order[n*n_src + s] = wide order index of pupil n seen from source s
+ *     (-1 where the source or the diffracted order is outside the NA circle).
+ * Outputs a0/ax/ay[c][n], n < ninput (ax, ay are zero where xinput == 0). */
+typedef struct {
+  int n_clips, n_src, ninput, n_order, n_order_narrow;
+  int lpx, lpy;
+  double k, dx, dy, z0, kx0, ky0;
+  int s_center;
+  const int* d_src_l;
+  const int* d_src_m;
+  const int* d_src_nidx_narrow;
+  const euv_c64* d_ax_vc;
+  const euv_c64* d_ax_ab;
+  const int* d_lin;
+  const int* d_min;
+  const int* d_xin;
+  const int* d_pair_order;
+} euv_m3d_desc;
+
+int euv_m3d_fit(const euv_m3d_desc* desc, const euv_c64* d_ax_wide, const euv_c64* d_fmask,
+                euv_c64* d_a0, euv_c64* d_ax, euv_c64* d_ay, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Building blocks, exported for tests and for callers composing their own
+ * pipelines. */
+
+/* C[b] = alpha*scale[b] * A[b] B[b] + beta C[b] + diag_add * I  (complex FP64,
+ * column-major, batched by element strides).  Replaces matproduct
+ * (header.h:1559-1619).  `d_scale` may be NULL (= 1).  If d_steps is not NULL
+ * and step >= d_steps[b], batch b instead copies A into C (M == N == K). */
+int euv_zgemm(int m, int n, int k, euv_c64 alpha, const double* d_scale, const euv_c64* d_a,
+              int lda, long long stride_a, const euv_c64* d_b, int ldb, long long stride_b,
+              euv_c64 beta, euv_c64* d_c, int ldc, long long stride_c, euv_c64 diag_add,
+              int batch, const int* d_steps, int step, void* stream);
+
+/* Batched LU with partial pivoting, in place (replaces the getrf branch of
+ * matinv, header.h:1518-1529).  d_ipiv[b][j] (0-based row swapped with j);
+ * d_info[b] = 0 or 1 + first zero pivot column. */
+size_t euv_lu_workspace_bytes(int n, int batch);
+int euv_lu_factor(int n, euv_c64* d_a, int lda, long long stride_a, int* d_ipiv, int* d_info,
+                  int batch, void* stream);
+/* Solve A X = B with the factors (replaces getrs, header.h:1531-1533). */
+int euv_lu_solve(int n, int nrhs, const euv_c64* d_lu, int lda, long long stride_a,
+                 const int* d_ipiv, euv_c64* d_b, int ldb, long long stride_b, int batch,
+                 void* stream);
+
+/* Matrix functions of a slice: for each b, C[b] = cos(sqrt(D) d[b]) and
+ * S[b] = sin(sqrt(D) d[b]) / sqrt(D), by Taylor series and double-angle steps.
+ * The outputs of absorberS0 / absorberS depend on their eigen-decomposition
+ * D = W diag(al^2) W^-1 only through these two entire functions of D. */
+size_t euv_matfun_workspace_bytes(int n, int batch);
+int euv_matfun_cs(int n, const euv_c64* d_d, const double* d_thick, euv_c64* d_cos,
+                  euv_c64* d_sin, int batch, int m_max, int precision, void* d_work,
+                  size_t work_bytes, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EUVL_B200_H */

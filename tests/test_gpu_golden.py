@@ -1,0 +1,58 @@
+"""The CUDA path at the reference configuration against the reference's own
+golden outputs (cnn/intensity/abbe/emint.csv, cnn/intensity/m3d/inputxx.csv),
+for the reference's mask.bin: NA 0.33, 2048 nm clip, N = 8705 orders.
+
+The golden files were written by a revision of the reference whose mask y-flip
+is one row off the shipped header.h:1159 (pattern row j reads mask row
+NDIVY-j, the row past the mask reading as absorber): SimConfig(yflip_offset=1)
+reproduces it.  They are printed with 6 significant digits."""
+import gzip
+import io
+import os
+
+import numpy as np
+import pytest
+
+from euvlitho_b200 import io as eio
+from euvlitho_b200.config import SimConfig
+
+pytestmark = [pytest.mark.gpu, pytest.mark.slow]
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+@pytest.fixture(scope="module")
+def golden(cuda):
+    import torch
+    from euvlitho_b200.engine import Plan
+    cfg = SimConfig(yflip_offset=1)
+    with gzip.open(os.path.join(GOLDEN, "ref_mask.bin.gz"), "rb") as fh:
+        bits = np.frombuffer(fh.read(), np.uint8).copy()
+    plan = Plan(cfg, device=cuda)
+    t = torch.from_numpy(bits[None])
+    img = plan.intensity(t).cpu().numpy()[0, 0]
+    res = plan.m3d(t)
+    torch.cuda.synchronize()
+    with gzip.open(os.path.join(GOLDEN, "ref_emint.csv.gz"), "rt") as fh:
+        gI = eio.read_emint(io.StringIO(fh.read()))
+    with gzip.open(os.path.join(GOLDEN, "ref_inputxx.csv.gz"), "rt") as fh:
+        gx = eio.read_inputxx(io.StringIO(fh.read()))
+    return plan, img, res, gI, gx
+
+
+def test_emint_golden(golden):
+    plan, img, res, gI, gx = golden
+    assert img.shape == gI.shape == (512, 512)
+    err = np.max(np.abs(img - gI)) / np.max(gI)
+    assert err < 2e-6, err  # print precision of emint.csv
+
+
+def test_inputxx_golden(golden):
+    plan, img, res, gI, gx = golden
+    xin = plan.xinput == 1
+    a0 = res["a0"][0].cpu().numpy()
+    ax = res["ax"][0].cpu().numpy()[xin]
+    ay = res["ay"][0].cpu().numpy()[xin]
+    assert len(a0) == len(gx["a0"]) == 1901 and len(ax) == len(gx["ax"])
+    for got, ref in ((a0, gx["a0"]), (ax, gx["ax"]), (ay, gx["ay"])):
+        err = np.max(np.abs(got - ref)) / np.max(np.abs(ref))
+        assert err < 1e-3, err

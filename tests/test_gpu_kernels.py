@@ -1,0 +1,151 @@
+"""Building blocks of libeuvl_b200.so on the GPU against NumPy FP64."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from euvlitho_b200 import _lib as L
+from oracle import euv_oracle as O
+from tests.helpers import flat_bits, random_mask, rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def _t(a, dev):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+
+
+def _colmajor(A):
+    """numpy [b][rows][cols] -> device buffer in column-major per matrix."""
+    return np.ascontiguousarray(np.swapaxes(A, -1, -2))
+
+
+def _from_colmajor(buf, rows, cols):
+    return np.swapaxes(buf.reshape(-1, cols, rows), -1, -2)
+
+
+def _stream():
+    import torch
+    return torch.cuda.current_stream().cuda_stream
+
+
+@pytest.mark.parametrize("m,n,k,batch", [(64, 64, 64, 1), (121, 121, 121, 3), (100, 37, 70, 2), (5, 200, 33, 4), (961, 961, 961, 1)])
+def test_zgemm(cuda, m, n, k, batch):
+    import torch
+    rng = np.random.default_rng(m + n + k)
+    A = rng.standard_normal((batch, m, k)) + 1j * rng.standard_normal((batch, m, k))
+    B = rng.standard_normal((batch, k, n)) + 1j * rng.standard_normal((batch, k, n))
+    Cm = rng.standard_normal((batch, m, n)) + 1j * rng.standard_normal((batch, m, n))
+    alpha, beta, diag = 0.7 - 0.2j, -0.3 + 0.5j, 0.25 + 1j
+    scale = rng.uniform(0.5, 2.0, batch)
+    dA, dB, dC = _t(_colmajor(A), cuda), _t(_colmajor(B), cuda), _t(_colmajor(Cm), cuda)
+    dS = _t(scale, cuda)
+    L.call("euv_zgemm", m, n, k, L.c64.of(alpha), dS.data_ptr(), dA.data_ptr(), m, m * k,
+           dB.data_ptr(), k, k * n, L.c64.of(beta), dC.data_ptr(), m, m * n, L.c64.of(diag), batch,
+           None, 0, _stream())
+    torch.cuda.synchronize()
+    got = _from_colmajor(dC.cpu().numpy(), m, n)
+    ref = alpha * scale[:, None, None] * (A @ B) + beta * Cm
+    for b in range(batch):
+        ref[b][np.arange(min(m, n)), np.arange(min(m, n))] += diag
+    assert rel_err(got, ref) < 1e-13
+
+
+def test_zgemm_step_copy(cuda):
+    import torch
+    n, batch = 70, 3
+    rng = np.random.default_rng(0)
+    A = rng.standard_normal((batch, n, n)) + 1j * rng.standard_normal((batch, n, n))
+    dA = _t(_colmajor(A), cuda)
+    dC = torch.zeros_like(dA)
+    steps = _t(np.array([0, 2, 1], np.int32), cuda)
+    L.call("euv_zgemm", n, n, n, L.c64.of(1.0), None, dA.data_ptr(), n, n * n, dA.data_ptr(), n,
+           n * n, L.c64.of(0), dC.data_ptr(), n, n * n, L.c64.of(0), batch, steps.data_ptr(), 1,
+           _stream())
+    torch.cuda.synchronize()
+    got = _from_colmajor(dC.cpu().numpy(), n, n)
+    assert rel_err(got[0], A[0]) == 0.0          # step 1 >= 0 steps: copy
+    assert rel_err(got[1], A[1] @ A[1]) < 1e-13  # active
+    assert rel_err(got[2], A[2]) == 0.0
+
+
+@pytest.mark.parametrize("n,nrhs,batch", [(1, 1, 1), (31, 5, 2), (121, 121, 4), (200, 17, 2), (961, 40, 2)])
+def test_lu_solve(cuda, n, nrhs, batch):
+    import torch
+    rng = np.random.default_rng(n)
+    A = rng.standard_normal((batch, n, n)) + 1j * rng.standard_normal((batch, n, n))
+    B = rng.standard_normal((batch, n, nrhs)) + 1j * rng.standard_normal((batch, n, nrhs))
+    dA, dB = _t(_colmajor(A), cuda), _t(_colmajor(B), cuda)
+    piv = torch.empty(batch * n, dtype=torch.int32, device=cuda)
+    info = torch.empty(batch, dtype=torch.int32, device=cuda)
+    L.call("euv_lu_factor", n, dA.data_ptr(), n, n * n, piv.data_ptr(), info.data_ptr(), batch, _stream())
+    L.call("euv_lu_solve", n, nrhs, dA.data_ptr(), n, n * n, piv.data_ptr(), dB.data_ptr(), n,
+           n * nrhs, batch, _stream())
+    torch.cuda.synchronize()
+    assert info.cpu().numpy().tolist() == [0] * batch
+    X = _from_colmajor(dB.cpu().numpy(), n, nrhs)
+    ref = np.linalg.solve(A, B)
+    assert rel_err(X, ref) < 1e-10
+
+
+def test_lu_reports_singular(cuda):
+    import torch
+    n = 40
+    A = np.zeros((1, n, n), complex)
+    A[0, :, :] = np.arange(n)[None, :]  # rank one
+    dA = _t(_colmajor(A), cuda)
+    piv = torch.empty(n, dtype=torch.int32, device=cuda)
+    info = torch.empty(1, dtype=torch.int32, device=cuda)
+    L.call("euv_lu_factor", n, dA.data_ptr(), n, n * n, piv.data_ptr(), info.data_ptr(), 1, _stream())
+    torch.cuda.synchronize()
+    assert info.item() > 0
+
+
+@pytest.mark.parametrize("n,d", [(121, 60.0), (121, 7.5), (300, 60.0)])
+def test_matfun_cos_sinc(cuda, n, d):
+    import torch
+    rng = np.random.default_rng(n)
+    k = 2 * np.pi / 13.5
+    # a D like the slice matrices: k^2 eps_avg - diag(kxy2) + small Toeplitz-like coupling
+    Dm = np.diag(k * k * (0.93 + 0.05j) - rng.uniform(0, 0.01, n)) + \
+        0.004 * (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))) / np.sqrt(n)
+    D = Dm[None]
+    dD = _t(_colmajor(D), cuda)
+    th = _t(np.array([d]), cuda)
+    dc, ds = torch.empty_like(dD), torch.empty_like(dD)
+    wb = L.lib().euv_matfun_workspace_bytes(n, 1)
+    ws = torch.empty(wb, dtype=torch.uint8, device=cuda)
+    L.call("euv_matfun_cs", n, dD.data_ptr(), th.data_ptr(), dc.data_ptr(), ds.data_ptr(), 1, 12,
+           L.EUV_PREC_FP64, ws.data_ptr(), wb, _stream())
+    torch.cuda.synchronize()
+    w, V = np.linalg.eig(Dm)
+    r = np.sqrt(w)
+    Vi = np.linalg.inv(V)
+    cref = (V * np.cos(r * d)) @ Vi
+    sref = (V * (np.sin(r * d) / r)) @ Vi
+    assert rel_err(_from_colmajor(dc.cpu().numpy(), n, n)[0], cref) < 1e-11
+    assert rel_err(_from_colmajor(ds.cpu().numpy(), n, n)[0], sref) < 1e-11
+
+
+@pytest.mark.parametrize("P,delta,lh,mh,vac", [(64, 1.0, 6, 6, 0), (64, 0.5, 4, 7, 1), (256, 1.0, 10, 10, 0)])
+def test_mask_spectrum(cuda, P, delta, lh, mh, vac):
+    import torch
+    from tests.helpers import packed
+    m2 = random_mask(P, P, seed=P + lh)
+    cfg = O.SimConfig(ndivx=P, ndivy=P, delta=delta)
+    ref = O.maskamp(flat_bits(m2), cfg, 0.0 if vac else 1.0, 1.0 if vac else 0.0, 0, 0)
+    # maskamp gives orders -2L..2L: call with L=lh/2 only when even; compute directly instead
+    pat = O.mask_pattern(flat_bits(m2), cfg, 0.0 if vac else 1.0, 1.0 if vac else 0.0)
+    F = np.fft.fft2(pat) / pat.size
+    ref = F[np.ix_(np.arange(-lh, lh + 1) % pat.shape[0], np.arange(-mh, mh + 1) % pat.shape[1])]
+    bits = _t(packed(m2), cuda)
+    out = torch.empty((2 * lh + 1) * (2 * mh + 1), dtype=torch.complex128, device=cuda)
+    fd = int(P / delta + 1e-6)
+    wb = L.lib().euv_mask_spectrum_workspace_bytes(1, P, P, fd, fd, lh, mh)
+    ws = torch.empty(wb, dtype=torch.uint8, device=cuda)
+    L.call("euv_mask_spectrum", bits.data_ptr(), 1, P, P, fd, fd, lh, mh, vac, 0, out.data_ptr(),
+           ws.data_ptr(), wb, _stream())
+    torch.cuda.synchronize()
+    got = out.cpu().numpy().reshape(2 * mh + 1, 2 * lh + 1).T
+    assert np.max(np.abs(got - ref)) < 1e-14
