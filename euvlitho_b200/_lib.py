@@ -23,7 +23,7 @@ EUV_PREC_MIXED = 1
 
 # Every symbol include/euvl_b200.h declares.
 EXPORTS = (
-    "euv_version", "euv_last_error",
+    "euv_version", "euv_last_error", "euv_kernel_launches",
     "euv_mask_spectrum_workspace_bytes", "euv_mask_spectrum",
     "euv_amp_workspace_bytes", "euv_amp",
     "euv_abbe", "euv_m3d_fit",
@@ -108,6 +108,7 @@ def _declare(lib: C.CDLL) -> None:
     i, d, sz, ll = C.c_int, C.c_double, C.c_size_t, C.c_longlong
     lib.euv_version.restype = C.c_char_p
     lib.euv_last_error.restype = C.c_char_p
+    lib.euv_kernel_launches.restype = C.c_ulonglong
     lib.euv_mask_spectrum_workspace_bytes.restype = sz
     lib.euv_mask_spectrum_workspace_bytes.argtypes = [i] * 7
     lib.euv_mask_spectrum.restype = i

@@ -184,8 +184,8 @@ extern "C" int euv_abbe(const euv_abbe_desc* d, const euv_c64* d_ax, double* d_i
     euv_set_error("euv_abbe: pupil too large for one CTA (%zu bytes of shared memory)", smem);
     return EUV_ERR_BAD_ARG;
   }
-  EUV_CUDA_TRY(cudaFuncSetAttribute(abbe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)smem));
+  static int smem_done[64];
+  EUV_CUDA_TRY(ensure_smem(abbe_kernel, (int)smem, smem_done));
   dim3 grid(ystripes, nsplit, d->n_units);
   abbe_kernel<<<grid, AB_THREADS, smem, stream>>>(p, reinterpret_cast<const double2*>(d_ax),
                                                   d_image);

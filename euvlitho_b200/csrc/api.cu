@@ -4,6 +4,13 @@
 #include "common.cuh"
 
 static thread_local char g_err[1024] = "";
+static unsigned long long g_launches = 0;
+
+extern "C" void euv_count_launch(void) { __atomic_fetch_add(&g_launches, 1ull, __ATOMIC_RELAXED); }
+
+extern "C" unsigned long long euv_kernel_launches(void) {
+  return __atomic_load_n(&g_launches, __ATOMIC_RELAXED);
+}
 
 extern "C" void euv_set_error(const char* fmt, ...) {
   va_list ap;

@@ -75,6 +75,29 @@ __host__ __device__ __forceinline__ cplx fromc(euv_c64 a) { return mk(a.re, a.im
     }                                                          \
   } while (0)
 
-#define EUV_LAUNCH_CHECK() EUV_CUDA_TRY(cudaGetLastError())
+// Every kernel launch of the library is followed by this check, which also
+// counts the launch (euv_kernel_launches()).
+#define EUV_LAUNCH_CHECK()        \
+  do {                            \
+    euv_count_launch();           \
+    EUV_CUDA_TRY(cudaGetLastError()); \
+  } while (0)
 
 extern "C" void euv_set_error(const char* fmt, ...);
+extern "C" void euv_count_launch(void);
+
+namespace euv {
+// Raise a kernel's dynamic shared-memory limit once per device (the first call
+// happens outside any stream capture; later calls do nothing).
+template <typename K>
+inline cudaError_t ensure_smem(K kernel, int bytes, int* done_per_device) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  if (__atomic_load_n(&done_per_device[dev], __ATOMIC_ACQUIRE) >= bytes) return cudaSuccess;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess) __atomic_store_n(&done_per_device[dev], bytes, __ATOMIC_RELEASE);
+  return e;
+}
+}  // namespace euv

@@ -185,8 +185,8 @@ __global__ void __launch_bounds__(GTHREADS, 2) zgemm_kernel(GemmArgs p) {
 
 int zgemm_launch(const GemmArgs& p, int batch, cudaStream_t stream) {
   if (p.m <= 0 || p.n <= 0 || batch <= 0) return EUV_OK;
-  EUV_CUDA_TRY(cudaFuncSetAttribute(zgemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)GSMEM));
+  static int smem_done[64];
+  EUV_CUDA_TRY(ensure_smem(zgemm_kernel, (int)GSMEM, smem_done));
   dim3 grid((p.m + GBM - 1) / GBM, (p.n + GBN - 1) / GBN, batch);
   zgemm_kernel<<<grid, GTHREADS, GSMEM, stream>>>(p);
   EUV_LAUNCH_CHECK();

@@ -112,6 +112,7 @@ class Plan:
         self._t_m = torch.tensor(mi, dtype=torch.int32, device=dev)
         self._abbe_tables = None
         self._m3d_tables = None
+        self._batches: Dict[Tuple[int, int], "IntensityBatch"] = {}
 
     # ------------------------------------------------------------ helpers
     def _i32(self, a) -> torch.Tensor:
@@ -264,46 +265,30 @@ class Plan:
         self._abbe_tables = tb
         return tb
 
-    def intensity(self, masks, out: Optional[torch.Tensor] = None) -> torch.Tensor:
-        """Abbe images [clips, pols, XDIV, YDIV] (intensity.cpp:219-408); I[x][y]."""
-        cfg = self.cfg
+    def intensity_batch(self, n_clips: int, n_mask_slices: int = 1) -> "IntensityBatch":
+        """Prepared launch for n_clips clips (cached per shape)."""
+        key = (n_clips, n_mask_slices)
+        b = self._batches.get(key)
+        if b is None:
+            b = IntensityBatch(self, n_clips, n_mask_slices)
+            self._batches[key] = b
+        return b
+
+    def intensity(self, masks, plain: bool = False) -> torch.Tensor:
+        """Abbe images [clips, pols, XDIV, YDIV] (intensity.cpp:219-408), I[x][y].
+
+        ``masks``: packed uint8 [clips, bytes] or [clips, slices, bytes], on the
+        host or the device.  ``plain=True`` runs one (clip, family,
+        polarisation) unit at a time (the unbatched FP64 form).  The result is
+        a new tensor."""
         m = self.as_mask_tensor(masks)
-        nc = m.shape[0]
-        tb = self.abbe_tables()
-        ntab = len(tb["pol"])
-        spec = self.spectra(m, 2 * self.orders.lmax, 2 * self.orders.mmax)
-        # units: clip-major, then (pol, family) table order
-        U = nc * ntab
-        tab = np.tile(np.arange(ntab, dtype=np.int32), nc)
-        clip = np.repeat(np.arange(nc, dtype=np.int32), ntab)
-        npol = len(self.pols)
-        nf = len(self.fams)
-        img = clip * npol + (tab // nf)
-        keep: list = []
-        desc = self.amp_desc(self.orders, self._t_l, self._t_m, self._f64(tb["kx0"][tab]),
-                             self._f64(tb["ky0"][tab]), self._i32(tb["pol"][tab]),
-                             self._i32(clip), self._i32(tb["order"][tab]),
-                             self._f64(tb["kz2"][tab]), keep)
-        ax = torch.empty((U, tb["n_src"], self.orders.n), dtype=torch.complex128, device=self.device)
-        self.run_amp(desc, spec, ax)
-        if out is None:
-            out = torch.zeros((nc, npol, cfg.xdiv, cfg.ydiv), dtype=torch.float64, device=self.device)
+        b = self.intensity_batch(m.shape[0], m.shape[1])
+        b.masks.copy_(m)
+        if plain:
+            b.run_plain()
         else:
-            out.zero_()
-        t_tab, t_img, t_ns = self._i32(tab), self._i32(img), self._i32(tb["nsrc"][tab])
-        inv_w = self._f64([1.0 / self.sdivsum] * (nc * npol))
-        ad = L.AbbeDesc()
-        ad.xdiv, ad.ydiv = cfg.xdiv, cfg.ydiv
-        ad.lpx, ad.lpy = cfg.lpmaxX, cfg.lpmaxY
-        ad.ncut, ad.n_units, ad.n_src, ad.n_order = self.ncut, U, tb["n_src"], self.orders.n
-        ad.d_coef, ad.d_nidx = _ptr(tb["coef"]), _ptr(tb["nidx"])
-        ad.d_px, ad.d_py, ad.d_row_start = _ptr(tb["px"]), _ptr(tb["py"]), _ptr(tb["row_start"])
-        ad.d_tab_of_unit, ad.d_img_of_unit, ad.d_nsrc_of_unit = _ptr(t_tab), _ptr(t_img), _ptr(t_ns)
-        ad.n_images = nc * npol
-        ad.d_inv_weight = _ptr(inv_w)
-        L.call("euv_abbe", C.byref(ad), ax.data_ptr(), out.data_ptr(), _stream())
-        self._last_keep = (keep, t_tab, t_img, t_ns, inv_w, ax)
-        return out
+            b.run()
+        return b.image.clone()
 
     # ------------------------------------------------------------ M3D
     def m3d_tables(self):
@@ -381,3 +366,134 @@ class Plan:
                axp.data_ptr(), ayp.data_ptr(), _stream())
         self._last_keep = (ax_wide, fmask)
         return {"a0": a0, "ax": axp, "ay": ayp, "Ax": ax_wide, "srcs": srcs}
+
+
+class IntensityBatch:
+    """Static buffers and descriptors for the Abbe images of ``n_clips`` clips.
+
+    ``run()`` enqueues, on the current stream, the mask spectra, the batched
+    ampS of every (clip, polarisation, family) unit and the fused Abbe kernel;
+    it allocates nothing and never synchronises, so it can be captured in a
+    CUDA graph (``capture()`` / ``replay()``).  ``run_plain()`` is the
+    unbatched FP64 form: one unit per ampS call."""
+
+    def __init__(self, plan: Plan, n_clips: int, n_mask_slices: int = 1):
+        cfg = plan.cfg
+        self.plan = plan
+        self.n_clips = nc = n_clips
+        dev = plan.device
+        tb = plan.abbe_tables()
+        self.tb = tb
+        ntab = len(tb["pol"])
+        self.U = U = nc * ntab
+        tab = np.tile(np.arange(ntab, dtype=np.int32), nc)
+        clip = np.repeat(np.arange(nc, dtype=np.int32), ntab)
+        npol = len(plan.pols)
+        nf = len(plan.fams)
+        img = clip * npol + (tab // nf)
+        self.masks = torch.zeros((nc, n_mask_slices, plan.mask_bytes()), dtype=torch.uint8, device=dev)
+        L_, M_ = plan.orders.lmax, plan.orders.mmax
+        self.lh, self.mh = 2 * L_, 2 * M_
+        self.spec_raw = torch.empty((nc * n_mask_slices, (2 * self.lh + 1) * (2 * self.mh + 1)),
+                                    dtype=torch.complex128, device=dev)
+        self.spec = self.spec_raw.view(nc, n_mask_slices, -1) if (n_mask_slices == cfg.nabs or cfg.nabs == 1) \
+            else torch.empty((nc, cfg.nabs, self.spec_raw.shape[1]), dtype=torch.complex128, device=dev)
+        self.ax = torch.empty((U, tb["n_src"], plan.orders.n), dtype=torch.complex128, device=dev)
+        self.image = torch.zeros((nc, npol, cfg.xdiv, cfg.ydiv), dtype=torch.float64, device=dev)
+        self.keep: list = []
+        self.t_kx0 = plan._f64(tb["kx0"][tab])
+        self.t_ky0 = plan._f64(tb["ky0"][tab])
+        self.t_pol = plan._i32(tb["pol"][tab])
+        self.t_clip = plan._i32(clip)
+        self.t_order = plan._i32(tb["order"][tab])
+        self.t_kz2 = plan._f64(tb["kz2"][tab])
+        self.desc = plan.amp_desc(plan.orders, plan._t_l, plan._t_m, self.t_kx0, self.t_ky0,
+                                  self.t_pol, self.t_clip, self.t_order, self.t_kz2, self.keep)
+        self.t_tab, self.t_img, self.t_ns = plan._i32(tab), plan._i32(img), plan._i32(tb["nsrc"][tab])
+        self.inv_w = plan._f64([1.0 / plan.sdivsum] * (nc * npol))
+        ad = L.AbbeDesc()
+        ad.xdiv, ad.ydiv = cfg.xdiv, cfg.ydiv
+        ad.lpx, ad.lpy = cfg.lpmaxX, cfg.lpmaxY
+        ad.ncut, ad.n_units, ad.n_src, ad.n_order = plan.ncut, U, tb["n_src"], plan.orders.n
+        ad.d_coef, ad.d_nidx = _ptr(tb["coef"]), _ptr(tb["nidx"])
+        ad.d_px, ad.d_py, ad.d_row_start = _ptr(tb["px"]), _ptr(tb["py"]), _ptr(tb["row_start"])
+        ad.d_tab_of_unit, ad.d_img_of_unit = _ptr(self.t_tab), _ptr(self.t_img)
+        ad.d_nsrc_of_unit = _ptr(self.t_ns)
+        ad.n_images = nc * npol
+        ad.d_inv_weight = _ptr(self.inv_w)
+        self.adesc = ad
+        lib = L.lib()
+        self.spec_bytes = lib.euv_mask_spectrum_workspace_bytes(nc * n_mask_slices, cfg.ndivx, cfg.ndivy,
+                                                               cfg.fdivx, cfg.fdivy, self.lh, self.mh)
+        self.amp_bytes = lib.euv_amp_workspace_bytes(C.byref(self.desc))
+        if self.amp_bytes == 0:
+            raise ValueError("invalid ampS descriptor")
+        self.work = torch.empty(max(self.spec_bytes, self.amp_bytes), dtype=torch.uint8, device=dev)
+        self.graph: Optional[torch.cuda.CUDAGraph] = None
+        self._plain = None
+
+    def _spectra(self) -> None:
+        cfg = self.plan.cfg
+        n = self.masks.shape[0] * self.masks.shape[1]
+        L.call("euv_mask_spectrum", self.masks.data_ptr(), n, cfg.ndivx, cfg.ndivy, cfg.fdivx,
+               cfg.fdivy, self.lh, self.mh, 0, cfg.yflip_offset, self.spec_raw.data_ptr(),
+               self.work.data_ptr(), self.work.numel(), _stream())
+        if self.spec.data_ptr() != self.spec_raw.data_ptr():
+            self.spec.copy_(self.spec_raw.view(self.n_clips, 1, -1).expand_as(self.spec))
+
+    def run(self) -> None:
+        self._spectra()
+        L.call("euv_amp", C.byref(self.desc), self.spec.data_ptr(), self.ax.data_ptr(),
+               self.work.data_ptr(), self.work.numel(), _stream())
+        self.image.zero_()
+        L.call("euv_abbe", C.byref(self.adesc), self.ax.data_ptr(), self.image.data_ptr(), _stream())
+
+    def _plain_descs(self):
+        if self._plain is not None:
+            return self._plain
+        descs = []
+        ns = self.ax.shape[1] * self.ax.shape[2]
+        for u in range(self.U):
+            d = L.AmpDesc.from_buffer_copy(self.desc)
+            d.n_units = 1
+            d.d_kx0 = self.t_kx0.data_ptr() + 8 * u
+            d.d_ky0 = self.t_ky0.data_ptr() + 8 * u
+            d.d_polar = self.t_pol.data_ptr() + 4 * u
+            d.d_spec = self.t_clip.data_ptr() + 4 * u
+            d.d_src_order = self.t_order.data_ptr() + 4 * u * self.desc.n_src
+            d.d_src_2kz = self.t_kz2.data_ptr() + 8 * u * self.desc.n_src
+            a = L.AbbeDesc.from_buffer_copy(self.adesc)
+            a.n_units = 1
+            a.d_tab_of_unit = self.t_tab.data_ptr() + 4 * u
+            a.d_img_of_unit = self.t_img.data_ptr() + 4 * u
+            a.d_nsrc_of_unit = self.t_ns.data_ptr() + 4 * u
+            descs.append((d, a, self.ax.data_ptr() + 16 * ns * u))
+        wb = L.lib().euv_amp_workspace_bytes(C.byref(descs[0][0]))
+        self._plain = (descs, wb)
+        return self._plain
+
+    def run_plain(self) -> None:
+        """The unbatched FP64 form: every unit solved and imaged on its own."""
+        descs, wb = self._plain_descs()
+        self._spectra()
+        self.image.zero_()
+        for d, a, axp in descs:
+            L.call("euv_amp", C.byref(d), self.spec.data_ptr(), axp, self.work.data_ptr(), wb, _stream())
+            L.call("euv_abbe", C.byref(a), axp, self.image.data_ptr(), _stream())
+
+    def capture(self) -> None:
+        """Capture run() into a CUDA graph (call run() once before, outside capture)."""
+        g = torch.cuda.CUDAGraph()
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            with torch.cuda.graph(g, stream=s):
+                self.run()
+        torch.cuda.current_stream().wait_stream(s)
+        self.graph = g
+
+    def replay(self) -> None:
+        if self.graph is None:
+            self.run()
+        else:
+            self.graph.replay()

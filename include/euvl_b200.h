@@ -57,9 +57,12 @@ typedef struct {
   int nml; /* Mo/Si periods (header.h NML) */
 } euv_stack;
 
-/* Library version and last error. */
+/* Library version, last error, and the number of kernels the library has
+ * enqueued in this process (launches captured into a CUDA graph count once,
+ * at capture). */
 const char* euv_version(void);
 const char* euv_last_error(void);
+unsigned long long euv_kernel_launches(void);
 
 /* ------------------------------------------------------------------------ */
 /* Mask spectrum: replaces maskamp (header.h:1147-1206) with fourier /

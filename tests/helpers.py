@@ -20,28 +20,9 @@ def to_oracle(cfg: SimConfig) -> O.SimConfig:
 
 
 def random_mask(ndivx: int, ndivy: int, seed: int, frac: float = 0.36) -> np.ndarray:
-    """Seeded layout of lines and contacts, 0/1 [ndivy][ndivx] (1 = vacuum).
-
-    Axis-aligned lines of width 16..64 nm at pitch 2-4x width plus square
-    contacts 16..64 nm, absorber area fraction around `frac`."""
-    rng = np.random.Generator(np.random.PCG64(seed))
-    m = np.ones((ndivy, ndivx), np.uint8)
-    vertical = rng.random() < 0.5
-    w = int(rng.integers(max(2, min(16, ndivx // 16)), max(3, min(64, ndivx // 4))))
-    pitch = int(w * rng.uniform(2.0, 4.0))
-    off = int(rng.integers(0, pitch))
-    n = ndivx if vertical else ndivy
-    for s in range(off, n, pitch):
-        if vertical:
-            m[:, s:s + w] = 0
-        else:
-            m[s:s + w, :] = 0
-    while (1.0 - m.mean()) < frac:
-        c = int(rng.integers(max(2, min(16, ndivx // 16)), max(3, min(64, ndivx // 4))))
-        x = int(rng.integers(0, ndivx - c))
-        y = int(rng.integers(0, ndivy - c))
-        m[y:y + c, x:x + c] = 0
-    return m
+    """Seeded lines-and-contacts layout, 0/1 [ndivy][ndivx] (1 = vacuum)."""
+    from euvlitho_b200.masks import synth_mask
+    return synth_mask(ndivx, ndivy, seed, frac)
 
 
 def packed(mask2d: np.ndarray) -> np.ndarray:
