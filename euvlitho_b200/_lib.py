@@ -20,6 +20,7 @@ EUV_ERR_SINGULAR = 4
 EUV_MAX_SLICES = 32
 EUV_PREC_FP64 = 0
 EUV_PREC_MIXED = 1
+EUV_NOALLOC_SCRATCH_BYTES = 16 * 1024 * 1024
 
 # Every symbol include/euvl_b200.h declares.
 EXPORTS = (
@@ -28,7 +29,7 @@ EXPORTS = (
     "euv_amp_workspace_bytes", "euv_amp",
     "euv_abbe", "euv_m3d_fit",
     "euv_zgemm", "euv_lu_workspace_bytes", "euv_lu_factor", "euv_lu_solve",
-    "euv_matfun_workspace_bytes", "euv_matfun_cs",
+    "euv_matfun_workspace_bytes", "euv_matfun_cs", "euv_matfun_cs_noalloc",
 )
 
 
@@ -133,6 +134,8 @@ def _declare(lib: C.CDLL) -> None:
     lib.euv_matfun_workspace_bytes.argtypes = [i, i]
     lib.euv_matfun_cs.restype = i
     lib.euv_matfun_cs.argtypes = [i, P, P, P, P, i, i, i, P, sz, P]
+    lib.euv_matfun_cs_noalloc.restype = i
+    lib.euv_matfun_cs_noalloc.argtypes = [i, P, P, P, P, i, i, P]
 
 
 def lib() -> C.CDLL:

@@ -857,3 +857,103 @@ extern "C" int euv_matfun_cs(int n, const euv_c64* d_d, const double* d_thick, e
   if (S != S0) EUV_CUDA_TRY(cudaMemcpyAsync(S0, S, nn * batch * sizeof(double2), cudaMemcpyDeviceToDevice, stream));
   return EUV_OK;
 }
+
+// ------------------------------------------------------------------ matfun, no allocation
+// Scratch of euv_matfun_cs_noalloc: a fixed device array in this library, so the
+// entry point needs no workspace from the caller and allocates nothing.  It is
+// EUV_NOALLOC_SCRATCH_BYTES on every GPU that loads the library, for the life of
+// the process.  Every call uses the same array.
+static __device__ __align__(256) unsigned char g_matfun_scratch[EUV_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+// Device address of g_matfun_scratch per device, looked up on the first call
+// made with that device current (cudaGetSymbolAddress is a host-side query).
+void* g_scratch_ptr[64];
+int g_scratch_ready[64];
+
+int scratch_for_current_device(void** out) {
+  int dev = 0;
+  EUV_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) {
+    euv_set_error("euv_matfun_cs_noalloc: device ordinal %d out of range", dev);
+    return EUV_ERR_BAD_ARG;
+  }
+  if (!__atomic_load_n(&g_scratch_ready[dev], __ATOMIC_ACQUIRE)) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_matfun_scratch);
+    if (e != cudaSuccess || p == nullptr) {
+      euv_set_error("euv_matfun_cs_noalloc: cudaGetSymbolAddress failed on device %d: %s", dev,
+                    cudaGetErrorString(e));
+      return EUV_ERR_CUDA;
+    }
+    g_scratch_ptr[dev] = p;
+    __atomic_store_n(&g_scratch_ready[dev], 1, __ATOMIC_RELEASE);
+  }
+  *out = g_scratch_ptr[dev];
+  return EUV_OK;
+}
+}  // namespace
+
+extern "C" int euv_matfun_cs_noalloc(int n, const euv_c64* d_d, const double* d_thick,
+                                     euv_c64* d_cos, euv_c64* d_sin, int batch, int m_max,
+                                     void* stream_) {
+  if (n <= 0 || batch <= 0 || !d_d || !d_thick || !d_cos || !d_sin || m_max < 0 ||
+      m_max > kMaxSteps) {
+    euv_set_error("euv_matfun_cs_noalloc: bad arguments");
+    return EUV_ERR_BAD_ARG;
+  }
+  size_t need;
+  {
+    Bump dry{nullptr, (size_t)-1, 0, true};
+    const long long nn0 = (long long)n * n;
+    for (int i = 0; i < 5; ++i) dry.take<double2>(nn0 * batch);
+    for (int i = 0; i < 4; ++i) dry.take<double>(batch);
+    dry.take<int>(batch);
+    dry.take<int>(1);
+    need = dry.off;
+  }
+  if (need > (size_t)EUV_NOALLOC_SCRATCH_BYTES) {
+    euv_set_error("euv_matfun_cs_noalloc: n=%d batch=%d needs %zu bytes of scratch, above the "
+                  "fixed %zu bytes (use euv_matfun_cs with a caller workspace)",
+                  n, batch, need, (size_t)EUV_NOALLOC_SCRATCH_BYTES);
+    return EUV_ERR_BAD_ARG;
+  }
+  void* scratch = nullptr;
+  int rc = scratch_for_current_device(&scratch);
+  if (rc) return rc;
+  cudaStream_t stream = (cudaStream_t)stream_;
+  const long long nn = (long long)n * n;
+  Bump bp{reinterpret_cast<char*>(scratch), (size_t)EUV_NOALLOC_SCRATCH_BYTES, 0, true};
+  MatfunBufs mb;
+  mb.P2 = bp.take<double2>(nn * batch);
+  mb.P3 = bp.take<double2>(nn * batch);
+  mb.P4 = bp.take<double2>(nn * batch);
+  mb.T1 = bp.take<double2>(nn * batch);
+  mb.T2 = bp.take<double2>(nn * batch);
+  mb.norm = bp.take<double>(batch);
+  mb.h = bp.take<double>(batch);
+  mb.h2 = bp.take<double>(batch);
+  mb.h4 = bp.take<double>(batch);
+  mb.steps = bp.take<int>(batch);
+  mb.capped = bp.take<int>(1);
+  if (!bp.ok) {
+    euv_set_error("euv_matfun_cs_noalloc: scratch layout overflow");
+    return EUV_ERR_BAD_ARG;
+  }
+  // The array keeps the previous call's contents: the only state that must
+  // start at zero is the cap flag (the column-norm maxima are cleared by matfun).
+  EUV_CUDA_TRY(cudaMemsetAsync(mb.capped, 0, sizeof(int), stream));
+  Gemm gemm{EUV_PREC_FP64, nullptr, 0, stream};
+  double2* C = reinterpret_cast<double2*>(d_cos);
+  double2* S = reinterpret_cast<double2*>(d_sin);
+  double2* C0 = C;
+  double2* S0 = S;
+  rc = matfun(n, batch, reinterpret_cast<const double2*>(d_d), d_thick, &C, &S, mb, m_max, gemm,
+              stream);
+  if (rc) return rc;
+  if (C != C0)
+    EUV_CUDA_TRY(cudaMemcpyAsync(C0, C, nn * batch * sizeof(double2), cudaMemcpyDeviceToDevice, stream));
+  if (S != S0)
+    EUV_CUDA_TRY(cudaMemcpyAsync(S0, S, nn * batch * sizeof(double2), cudaMemcpyDeviceToDevice, stream));
+  return EUV_OK;
+}

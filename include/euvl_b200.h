@@ -234,6 +234,32 @@ int euv_matfun_cs(int n, const euv_c64* d_d, const double* d_thick, euv_c64* d_c
                   euv_c64* d_sin, int batch, int m_max, int precision, void* d_work,
                   size_t work_bytes, void* stream);
 
+/* Same as euv_matfun_cs (FP64), but without a workspace: no counterpart in
+ * the reference, which allocates on every call.
+ *
+ * For callers that cannot allocate device memory: code that runs while a
+ * framework captures a CUDA graph and forbids allocation inside the capture,
+ * plug-ins whose host application owns all device memory through its own
+ * allocator, and latency-critical loops that must not call cudaMalloc/cudaFree
+ * because those calls can synchronise the whole device.  The caller passes
+ * only the inputs and outputs; the scratch space is a fixed array of
+ * EUV_NOALLOC_SCRATCH_BYTES (16 MiB) inside the library, resident on every GPU
+ * that loads it until the process exits.  The function calls no allocator.
+ *
+ *  - Limit: 5*n*n*batch*16 bytes (+ a few hundred) must fit in the array, e.g.
+ *    n = 121 up to batch 14, n = 256 up to batch 3.  Larger requests return
+ *    EUV_ERR_BAD_ARG with a message and launch nothing.
+ *  - The first call on each device looks up the array's device address
+ *    (cudaGetSymbolAddress, with that device current); make that first call
+ *    before any stream capture.
+ *  - All calls share the one array and it keeps the last call's contents (the
+ *    function clears what must start at zero).  Calls whose GPU work overlaps,
+ *    e.g. on two streams at once, race on it: order them on one stream or
+ *    with events. */
+#define EUV_NOALLOC_SCRATCH_BYTES (16u * 1024u * 1024u)
+int euv_matfun_cs_noalloc(int n, const euv_c64* d_d, const double* d_thick, euv_c64* d_cos,
+                          euv_c64* d_sin, int batch, int m_max, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
