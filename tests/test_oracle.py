@@ -118,5 +118,9 @@ def test_pin_summary_within_print_precision():
         pytest.skip("pin not run yet")
     s = json.load(open(p))
     assert s["inputlm_equal"]
-    assert s["emint_max_abs_err_over_max"] < 1e-4
-    assert s["a0_max_abs_err_over_max"] < 1e-3
+    assert s["emint_max_abs_err_over_max"] < 2e-6  # print precision of emint.csv
+    # inputxx: the golden run read undefined memory for one mask row of the thin
+    # mask and of the uniform-mask solves; what is reproducible agrees to:
+    assert s["a0_max_abs_err_over_max"] < 4e-3
+    assert s["ax_max_abs_err_over_max"] < 1e-3 and s["ay_max_abs_err_over_max"] < 1e-3
+    assert s["a0_median_abs_err"] < 5e-6
