@@ -1,18 +1,526 @@
-// Mixed-precision complex GEMM (bulk products of the mixed form).
+// Mixed-precision complex GEMM on the 5th-generation tensor cores (tcgen05).
+//
+// C = alpha*scale[b] * A B + beta C + diag*I for complex FP64 A (MxK), B (KxN),
+// C (MxN), column-major and batched, computed as TF32x3: every FP64 real
+// operand is split into two TF32 values x = hi + lo (hi = x rounded to TF32,
+// lo = x - hi), and each real product is hi*hi + hi*lo + lo*hi with FP32
+// accumulation in tensor memory.  The complex product uses four real products:
+//   Re = ArBr - AiBi,  Im = ArBi + AiBr   (the minus sign through the MMA's
+//   negate-A bit), so one K step issues 12 tcgen05.mma into two accumulators.
+// Error per product ~1e-6 relative: the bulk products of the slab matrix
+// functions tolerate it (intensity error < 1e-4, see the tests); the interface
+// solves stay FP64.
+//
+// Operands are first rewritten (split_*_kernel) as four fp32 planes
+// [batch][Re_hi, Re_lo, Im_hi, Im_lo][rows][Kp] with K contiguous (K-major for
+// both A and B), Kp = K rounded up to 16.  The GEMM kernel:
+//   warp 0     : TMA producer (3-D tensor maps, 64-byte swizzle, 2 stages of
+//                4x(128x16) A + 4x(256x16) B fp32 = 96 KB);
+//   warp 1     : TMEM allocation (512 columns: Re and Im accumulators of a
+//                128x256 tile) and the single-thread MMA issue loop;
+//   warps 2..5 : epilogue, tcgen05.ld of their 32 TMEM lanes (= rows), complex
+//                FP64 result written column by column (coalesced).
+// All waits are bounded (about 2 s); a timeout sets the error word, drains the
+// copies and MMAs in flight, frees TMEM and returns.
+#include <cuda.h>
 #include "common.cuh"
 
 namespace euv {
 
-size_t gemm_mixed_workspace_bytes(int m, int n, int k, int batch) {
-  (void)m; (void)n; (void)k; (void)batch;
-  return 0;
+int zgemm(int m, int n, int k, cplx alpha, const double* scale, const double2* a, long long lda,
+          long long sa, const double2* b, long long ldb, long long sb, cplx beta, double2* c,
+          long long ldc, long long sc, cplx diag, int batch, const int* steps, int step,
+          cudaStream_t stream);
+
+constexpr int MX_BM = 128;
+constexpr int MX_BN = 256;
+constexpr int MX_BK = 16;  // fp32 elements: 64-byte rows, one 64B swizzle span
+constexpr int MX_STAGES = 2;
+constexpr int MX_PLANES = 4;
+constexpr int MX_A_TILE = MX_BM * MX_BK * 4;  // 8 KB
+constexpr int MX_B_TILE = MX_BN * MX_BK * 4;  // 16 KB
+constexpr int MX_STAGE_BYTES = MX_PLANES * (MX_A_TILE + MX_B_TILE);  // 96 KB
+constexpr int MX_THREADS = 192;
+constexpr int MX_TMEM_COLS = 512;
+constexpr size_t MX_SMEM = (size_t)MX_STAGES * MX_STAGE_BYTES + 1024 + 256;
+constexpr unsigned long long MX_TIMEOUT_NS = 2000000000ull;
+
+struct MixedArgs {
+  int m, n, kp;
+  double2 alpha, beta, diag;
+  const double* scale;
+  const double2* a;  // original FP64 A (copy mode)
+  long long lda, sa;
+  double2* c;
+  long long ldc, sc;
+  const int* steps;
+  int step;
+  int* err;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ unsigned long long globaltimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait: false after the deadline (or when another role already gave up).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
+                                          int* err) {
+  const unsigned long long t0 = globaltimer();
+  for (uint32_t it = 0;; ++it) {
+    if (mbar_try(bar, parity)) return true;
+    if ((it & 255u) == 255u) {
+      if (*abort_flag) return false;
+      if (globaltimer() - t0 > MX_TIMEOUT_NS) {
+        *abort_flag = 1;
+        atomicExch(err, 1);
+        return false;
+      }
+    }
+  }
+}
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z,
+                                            uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+// K-major operand, 64-byte swizzle: 8-row atoms of 512 B (SBO), version 1.
+__device__ __forceinline__ uint64_t umma_desc_sw64(const void* tile) {
+  const uint64_t addr = smem_u32(tile);
+  uint64_t d = 0;
+  d |= (addr >> 4) & 0x3FFFull;          // start address
+  d |= (uint64_t)1 << 16;                // leading byte offset (unused for swizzled K-major)
+  d |= (uint64_t)(512 >> 4) << 32;       // stride byte offset: 8 rows x 64 B
+  d |= (uint64_t)1 << 46;                // descriptor version (sm_100)
+  d |= (uint64_t)4 << 61;                // SWIZZLE_64B
+  return d;
+}
+__device__ __forceinline__ constexpr uint32_t idesc_tf32(bool neg_a) {
+  return (1u << 4)                       // D: F32
+         | (2u << 7) | (2u << 10)        // A, B: TF32
+         | ((neg_a ? 1u : 0u) << 13)     // negate A
+         | ((uint32_t)(MX_BN >> 3) << 17) // N
+         | ((uint32_t)(MX_BM >> 4) << 24);// M
+}
+__device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc,
+                                          uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,"
+      "%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_ld_wait() {
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-int gemm_mixed(int, int, int, cplx, const double*, const double2*, long long, long long,
-               const double2*, long long, long long, cplx, double2*, long long, long long, cplx,
-               int, const int*, int, void*, size_t, cudaStream_t) {
-  euv_set_error("mixed precision GEMM is not available in this build");
-  return EUV_ERR_BAD_ARG;
+__global__ void __launch_bounds__(MX_THREADS, 1)
+    gemm_tf32x3_kernel(const __grid_constant__ CUtensorMap tmA,
+                       const __grid_constant__ CUtensorMap tmB, MixedArgs p) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + MX_STAGES * MX_STAGE_BYTES);
+  uint64_t* empty = full + MX_STAGES;
+  uint64_t* accum = empty + MX_STAGES;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accum + 1);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int b = blockIdx.z;
+  const int m0 = blockIdx.x * MX_BM, n0 = blockIdx.y * MX_BN;
+  double2* C = p.c + (long long)b * p.sc;
+
+  if (p.steps != nullptr && p.step >= p.steps[b]) {
+    // inactive double-angle step of this batch entry: C = A on this tile
+    const double2* A = p.a + (long long)b * p.sa;
+    for (int idx = threadIdx.x; idx < MX_BM * MX_BN; idx += MX_THREADS) {
+      int i = idx % MX_BM, j = idx / MX_BM;
+      int gi = m0 + i, gj = n0 + j;
+      if (gi < p.m && gj < p.n) C[gi + (long long)gj * p.ldc] = A[gi + (long long)gj * p.lda];
+    }
+    return;
+  }
+
+  auto a_tile = [&](int s, int pl) { return smem + s * MX_STAGE_BYTES + pl * MX_A_TILE; };
+  auto b_tile = [&](int s, int pl) {
+    return smem + s * MX_STAGE_BYTES + MX_PLANES * MX_A_TILE + pl * MX_B_TILE;
+  };
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < MX_STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(accum, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tmem_slot)),
+                 "r"(MX_TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const int nkb = p.kp / MX_BK;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      int issued = 0;
+      for (int kb = 0; kb < nkb; ++kb) {
+        const int s = kb % MX_STAGES;
+        const uint32_t ph = (uint32_t)((kb / MX_STAGES) & 1);
+        if (!mbar_wait(&empty[s], ph ^ 1u, abort_flag, p.err)) break;
+        mbar_expect_tx(&full[s], (uint32_t)MX_STAGE_BYTES);
+        const int k0 = kb * MX_BK;
+        for (int pl = 0; pl < MX_PLANES; ++pl)
+          tma_load_3d(a_tile(s, pl), &tmA, k0, m0, b * MX_PLANES + pl, &full[s]);
+        for (int pl = 0; pl < MX_PLANES; ++pl)
+          tma_load_3d(b_tile(s, pl), &tmB, k0, n0, b * MX_PLANES + pl, &full[s]);
+        issued = kb + 1;
+      }
+      if (*abort_flag) {
+        // drain this thread's copies in flight (bounded) before the CTA exits
+        for (int kb = (issued > MX_STAGES ? issued - MX_STAGES : 0); kb < issued; ++kb) {
+          const unsigned long long t0 = globaltimer();
+          while (!mbar_try(&full[kb % MX_STAGES], (uint32_t)((kb / MX_STAGES) & 1)) &&
+                 globaltimer() - t0 < MX_TIMEOUT_NS) {
+          }
+        }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      // (A plane, B plane, negate A) for Re and Im; planes: 0 Re_hi 1 Re_lo 2 Im_hi 3 Im_lo
+      const int re_a[6] = {0, 0, 1, 2, 2, 3}, re_b[6] = {0, 1, 0, 2, 3, 2};
+      const int im_a[6] = {0, 0, 1, 2, 2, 3}, im_b[6] = {2, 3, 2, 0, 1, 0};
+      const uint32_t id_pos = idesc_tf32(false), id_neg = idesc_tf32(true);
+      const uint32_t t_re = tmem, t_im = tmem + (uint32_t)MX_BN;
+      for (int kb = 0; kb < nkb; ++kb) {
+        const int s = kb % MX_STAGES;
+        const uint32_t ph = (uint32_t)((kb / MX_STAGES) & 1);
+        if (!mbar_wait(&full[s], ph, abort_flag, p.err)) break;
+        tc_fence_after();
+#pragma unroll
+        for (int k8 = 0; k8 < MX_BK / 8; ++k8) {
+#pragma unroll
+          for (int q = 0; q < 6; ++q) {
+            const uint64_t da = umma_desc_sw64(a_tile(s, re_a[q]) + k8 * 32);
+            const uint64_t db = umma_desc_sw64(b_tile(s, re_b[q]) + k8 * 32);
+            umma_tf32(t_re, da, db, q >= 3 ? id_neg : id_pos, (kb | k8 | q) ? 1u : 0u);
+          }
+#pragma unroll
+          for (int q = 0; q < 6; ++q) {
+            const uint64_t da = umma_desc_sw64(a_tile(s, im_a[q]) + k8 * 32);
+            const uint64_t db = umma_desc_sw64(b_tile(s, im_b[q]) + k8 * 32);
+            umma_tf32(t_im, da, db, id_pos, (kb | k8 | q) ? 1u : 0u);
+          }
+        }
+        umma_commit(&empty[s]);  // frees the stage when these MMAs complete
+      }
+      umma_commit(accum);  // always: the epilogue / teardown waits on it
+    }
+  } else {
+    // epilogue: warps 2..5 read TMEM lanes (warp % 4) * 32 .. +31 = tile rows
+    const int q = warp & 3;
+    const bool waited = mbar_wait(accum, 0u, abort_flag, p.err) && !*abort_flag && nkb > 0;
+    const bool ok = __all_sync(0xffffffffu, waited);  // tcgen05.ld below is warp-collective
+    tc_fence_after();
+    const int row = m0 + q * 32 + lane;
+    const double sc = p.scale ? p.scale[b] : 1.0;
+    const cplx alpha = mk(p.alpha.x * sc, p.alpha.y * sc);
+    const cplx beta = mk(p.beta.x, p.beta.y);
+    const bool use_beta = (p.beta.x != 0.0 || p.beta.y != 0.0);
+    const cplx dg = mk(p.diag.x, p.diag.y);
+    if (ok) {
+      for (int c0 = 0; c0 < MX_BN; c0 += 16) {
+        if (n0 + c0 >= p.n) break;  // warp-uniform
+        uint32_t vr[16], vi[16];
+        const uint32_t lane_addr = ((uint32_t)(q * 32) << 16);
+        tmem_ld16(tmem + lane_addr + (uint32_t)c0, vr);
+        tmem_ld16(tmem + lane_addr + (uint32_t)(MX_BN + c0), vi);
+        tmem_ld_wait();
+        if (row < p.m) {
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            const int col = n0 + c0 + j;
+            if (col < p.n) {
+              double2* cp = C + row + (long long)col * p.ldc;
+              cplx v = alpha * mk((double)__uint_as_float(vr[j]), (double)__uint_as_float(vi[j]));
+              if (use_beta) {
+                double2 o = *cp;
+                v = v + beta * mk(o.x, o.y);
+              }
+              if (row == col) v = v + dg;
+              *cp = make_double2(v.x, v.y);
+            }
+          }
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    if (*abort_flag) {
+      // the MMAs in flight must finish before their TMEM is released (bounded)
+      const unsigned long long t0 = globaltimer();
+      while (!mbar_try(accum, 0u) && globaltimer() - t0 < MX_TIMEOUT_NS) {
+      }
+    }
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(MX_TMEM_COLS)
+                 : "memory");
+  }
+}
+
+__device__ __forceinline__ void split_tf32(double x, float& hi, float& lo) {
+  const float f = (float)x;
+  uint32_t h;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(f));
+  hi = __uint_as_float(h);
+  lo = (float)(x - (double)hi);
+}
+
+// A (col-major complex M x K) -> planes [b][4][M][Kp], K contiguous (transpose
+// through a 32x32 shared tile).
+__global__ void split_a_kernel(int M, int K, int Kp, const double2* A, long long lda,
+                               long long sa, float* out) {
+  __shared__ double2 tile[32][33];
+  const int b = blockIdx.z;
+  const int m0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
+  A += (long long)b * sa;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  for (int j = ty; j < 32; j += 8) {
+    const int m = m0 + tx, k = k0 + j;
+    tile[j][tx] = (m < M && k < K) ? A[m + (long long)k * lda] : make_double2(0.0, 0.0);
+  }
+  __syncthreads();
+  const long long plane = (long long)M * Kp;
+  float* o = out + (long long)b * MX_PLANES * plane;
+  for (int j = ty; j < 32; j += 8) {
+    const int m = m0 + j, k = k0 + tx;
+    if (m < M && k < Kp) {
+      const double2 v = tile[tx][j];
+      float rh, rl, ih, il;
+      split_tf32(v.x, rh, rl);
+      split_tf32(v.y, ih, il);
+      const long long off = (long long)m * Kp + k;
+      o[off] = rh;
+      o[plane + off] = rl;
+      o[2 * plane + off] = ih;
+      o[3 * plane + off] = il;
+    }
+  }
+}
+
+// B (col-major complex K x N) -> planes [b][4][N][Kp], K contiguous.
+__global__ void split_b_kernel(int K, int N, int Kp, const double2* B, long long ldb,
+                               long long sb, float* out) {
+  const int b = blockIdx.y;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)N * Kp) return;
+  const int k = (int)(t % Kp), n = (int)(t / Kp);
+  B += (long long)b * sb;
+  const double2 v = k < K ? B[k + (long long)n * ldb] : make_double2(0.0, 0.0);
+  float rh, rl, ih, il;
+  split_tf32(v.x, rh, rl);
+  split_tf32(v.y, ih, il);
+  const long long plane = (long long)N * Kp;
+  float* o = out + (long long)b * MX_PLANES * plane;
+  o[t] = rh;
+  o[plane + t] = rl;
+  o[2 * plane + t] = ih;
+  o[3 * plane + t] = il;
+}
+
+// ------------------------------------------------------------------ host
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+// planes tensor [batch*4][rows][kp] fp32 -> 3-D map (kp, rows, batch*4), box (16, box_rows, 1)
+static int make_map(CUtensorMap* map, float* base, int rows, int kp, int nplanes, int box_rows) {
+  EncodeTiledFn enc = encode_fn();
+  if (!enc) {
+    euv_set_error("cuTensorMapEncodeTiled is not available from the driver");
+    return EUV_ERR_CUDA;
+  }
+  cuuint64_t dims[3] = {(cuuint64_t)kp, (cuuint64_t)rows, (cuuint64_t)nplanes};
+  cuuint64_t strides[2] = {(cuuint64_t)kp * 4, (cuuint64_t)kp * 4 * rows};
+  cuuint32_t box[3] = {(cuuint32_t)MX_BK, (cuuint32_t)box_rows, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    euv_set_error("cuTensorMapEncodeTiled failed (%d) rows=%d kp=%d", (int)r, rows, kp);
+    return EUV_ERR_CUDA;
+  }
+  return EUV_OK;
+}
+
+static inline int round_up(int x, int a) { return (x + a - 1) / a * a; }
+
+size_t gemm_mixed_workspace_bytes(int m, int n, int k, int batch) {
+  const size_t kp = (size_t)round_up(k > 0 ? k : 1, MX_BK);
+  size_t a = (size_t)batch * MX_PLANES * (size_t)m * kp * 4;
+  size_t b = (size_t)batch * MX_PLANES * (size_t)n * kp * 4;
+  a = (a + 1023) & ~(size_t)1023;
+  b = (b + 1023) & ~(size_t)1023;
+  return a + b + 1024;
+}
+
+int gemm_mixed(int m, int n, int k, cplx alpha, const double* scale, const double2* a,
+               long long lda, long long sa, const double2* b, long long ldb, long long sb,
+               cplx beta, double2* c, long long ldc, long long sc, cplx diag, int batch,
+               const int* steps, int step, void* work, size_t work_bytes, cudaStream_t stream) {
+  if (m <= 0 || n <= 0 || batch <= 0) return EUV_OK;
+  if (k <= 0 || batch > 65535 || (size_t)batch * MX_PLANES > 0x7fffffff) {
+    euv_set_error("gemm_mixed: unsupported shape");
+    return EUV_ERR_BAD_ARG;
+  }
+  const int kp = round_up(k, MX_BK);
+  const size_t need = gemm_mixed_workspace_bytes(m, n, k, batch);
+  if (work == nullptr || work_bytes < need ||
+      (reinterpret_cast<uintptr_t>(work) & 255u) != 0) {
+    euv_set_error("gemm_mixed: workspace too small or misaligned (%zu < %zu)", work_bytes, need);
+    return EUV_ERR_WORKSPACE;
+  }
+  char* w = reinterpret_cast<char*>(work);
+  float* pa = reinterpret_cast<float*>(w);
+  size_t abytes = ((size_t)batch * MX_PLANES * (size_t)m * kp * 4 + 1023) & ~(size_t)1023;
+  float* pb = reinterpret_cast<float*>(w + abytes);
+  size_t bbytes = ((size_t)batch * MX_PLANES * (size_t)n * kp * 4 + 1023) & ~(size_t)1023;
+  int* err = reinterpret_cast<int*>(w + abytes + bbytes);
+  EUV_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int), stream));
+  {
+    dim3 g((m + 31) / 32, (kp + 31) / 32, batch), t(32, 8);
+    split_a_kernel<<<g, t, 0, stream>>>(m, k, kp, a, lda, sa, pa);
+    EUV_LAUNCH_CHECK();
+    dim3 gb((unsigned)(((long long)n * kp + 255) / 256), batch);
+    split_b_kernel<<<gb, 256, 0, stream>>>(k, n, kp, b, ldb, sb, pb);
+    EUV_LAUNCH_CHECK();
+  }
+  CUtensorMap ta, tb;
+  int rc = make_map(&ta, pa, m, kp, batch * MX_PLANES, MX_BM);
+  if (rc) return rc;
+  rc = make_map(&tb, pb, n, kp, batch * MX_PLANES, MX_BN);
+  if (rc) return rc;
+  static int smem_done[64];
+  EUV_CUDA_TRY(ensure_smem(gemm_tf32x3_kernel, (int)MX_SMEM, smem_done));
+  MixedArgs p;
+  p.m = m;
+  p.n = n;
+  p.kp = kp;
+  p.alpha = make_double2(alpha.x, alpha.y);
+  p.beta = make_double2(beta.x, beta.y);
+  p.diag = make_double2(diag.x, diag.y);
+  p.scale = scale;
+  p.a = a;
+  p.lda = lda;
+  p.sa = sa;
+  p.c = c;
+  p.ldc = ldc;
+  p.sc = sc;
+  p.steps = steps;
+  p.step = step;
+  p.err = err;
+  dim3 grid((m + MX_BM - 1) / MX_BM, (n + MX_BN - 1) / MX_BN, batch);
+  gemm_tf32x3_kernel<<<grid, MX_THREADS, MX_SMEM, stream>>>(ta, tb, p);
+  EUV_LAUNCH_CHECK();
+  return EUV_OK;
 }
 
 }  // namespace euv
+
+using namespace euv;
+
+extern "C" size_t euv_zgemm_tf32x3_workspace_bytes(int m, int n, int k, int batch) {
+  if (m <= 0 || n <= 0 || k <= 0 || batch <= 0) return 0;
+  return gemm_mixed_workspace_bytes(m, n, k, batch);
+}
+
+extern "C" int euv_zgemm_tf32x3(int m, int n, int k, euv_c64 alpha, const double* d_scale,
+                                const euv_c64* d_a, int lda, long long stride_a,
+                                const euv_c64* d_b, int ldb, long long stride_b, euv_c64 beta,
+                                euv_c64* d_c, int ldc, long long stride_c, euv_c64 diag,
+                                int batch, const int* d_steps, int step, void* d_work,
+                                size_t work_bytes, void* stream) {
+  if (m <= 0 || n <= 0 || k <= 0 || batch <= 0 || lda < m || ldc < m || ldb < k || !d_a ||
+      !d_b || !d_c || (d_steps != nullptr && (m != n || m != k))) {
+    euv_set_error("euv_zgemm_tf32x3: bad arguments (m=%d n=%d k=%d)", m, n, k);
+    return EUV_ERR_BAD_ARG;
+  }
+  return gemm_mixed(m, n, k, fromc(alpha), d_scale, reinterpret_cast<const double2*>(d_a), lda,
+                    stride_a, reinterpret_cast<const double2*>(d_b), ldb, stride_b, fromc(beta),
+                    reinterpret_cast<double2*>(d_c), ldc, stride_c, fromc(diag), batch, d_steps,
+                    step, d_work, work_bytes, (cudaStream_t)stream);
+}

@@ -43,7 +43,7 @@ extern "C" {
 #define EUV_MAX_SLICES 32
 
 #define EUV_PREC_FP64 0  /* every product in FP64 */
-#define EUV_PREC_MIXED 1 /* bulk products on BF16x3 tensor cores, FP64 solves */
+#define EUV_PREC_MIXED 1 /* bulk products as TF32x3 on tcgen05 tensor cores, FP64 solves */
 
 typedef struct {
   double re, im;
@@ -213,6 +213,17 @@ int euv_zgemm(int m, int n, int k, euv_c64 alpha, const double* d_scale, const e
               int lda, long long stride_a, const euv_c64* d_b, int ldb, long long stride_b,
               euv_c64 beta, euv_c64* d_c, int ldc, long long stride_c, euv_c64 diag_add,
               int batch, const int* d_steps, int step, void* stream);
+
+/* The bulk product of EUV_PREC_MIXED: same contract as euv_zgemm, computed on
+ * the tcgen05 tensor cores as TF32x3 (each FP64 operand split into two TF32
+ * terms, three TF32 products per real product, FP32 accumulation; ~1e-6
+ * relative error per product).  Needs a workspace for the split operands. */
+size_t euv_zgemm_tf32x3_workspace_bytes(int m, int n, int k, int batch);
+int euv_zgemm_tf32x3(int m, int n, int k, euv_c64 alpha, const double* d_scale,
+                     const euv_c64* d_a, int lda, long long stride_a, const euv_c64* d_b, int ldb,
+                     long long stride_b, euv_c64 beta, euv_c64* d_c, int ldc, long long stride_c,
+                     euv_c64 diag, int batch, const int* d_steps, int step, void* d_work,
+                     size_t work_bytes, void* stream);
 
 /* Batched LU with partial pivoting, in place (replaces the getrf branch of
  * matinv, header.h:1518-1529).  d_ipiv[b][j] (0-based row swapped with j);

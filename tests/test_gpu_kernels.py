@@ -149,3 +149,68 @@ def test_mask_spectrum(cuda, P, delta, lh, mh, vac):
     torch.cuda.synchronize()
     got = out.cpu().numpy().reshape(2 * mh + 1, 2 * lh + 1).T
     assert np.max(np.abs(got - ref)) < 1e-14
+
+
+@pytest.mark.parametrize("m,n,k,batch", [(128, 256, 16, 1), (121, 121, 121, 2), (300, 200, 77, 2), (961, 961, 961, 2)])
+def test_zgemm_tf32x3(cuda, m, n, k, batch):
+    """tcgen05 TF32x3 complex GEMM against NumPy FP64.  The bound is set by the
+    FP32 accumulation in tensor memory (grows with K: ~1.5e-5 at K = 961)."""
+    import torch
+    rng = np.random.default_rng(7 * m + n + k)
+    A = rng.standard_normal((batch, m, k)) + 1j * rng.standard_normal((batch, m, k))
+    B = rng.standard_normal((batch, k, n)) + 1j * rng.standard_normal((batch, k, n))
+    Cm = rng.standard_normal((batch, m, n)) + 1j * rng.standard_normal((batch, m, n))
+    alpha, beta, diag = 0.5 + 0.25j, 0.3 - 0.1j, -1.0 + 0.0j
+    dA, dB, dC = _t(_colmajor(A), cuda), _t(_colmajor(B), cuda), _t(_colmajor(Cm), cuda)
+    wb = L.lib().euv_zgemm_tf32x3_workspace_bytes(m, n, k, batch)
+    ws = torch.empty(wb, dtype=torch.uint8, device=cuda)
+    L.call("euv_zgemm_tf32x3", m, n, k, L.c64.of(alpha), None, dA.data_ptr(), m, m * k,
+           dB.data_ptr(), k, k * n, L.c64.of(beta), dC.data_ptr(), m, m * n, L.c64.of(diag), batch,
+           None, 0, ws.data_ptr(), wb, _stream())
+    torch.cuda.synchronize()
+    got = _from_colmajor(dC.cpu().numpy(), m, n)
+    ref = alpha * (A @ B) + beta * Cm
+    for b in range(batch):
+        ref[b][np.arange(min(m, n)), np.arange(min(m, n))] += diag
+    assert rel_err(got, ref) < 3e-8 * k + 1e-6
+
+
+def test_zgemm_tf32x3_step_copy(cuda):
+    import torch
+    n, batch = 130, 2
+    rng = np.random.default_rng(1)
+    A = rng.standard_normal((batch, n, n)) + 1j * rng.standard_normal((batch, n, n))
+    dA = _t(_colmajor(A), cuda)
+    dC = torch.zeros_like(dA)
+    steps = _t(np.array([0, 3], np.int32), cuda)
+    wb = L.lib().euv_zgemm_tf32x3_workspace_bytes(n, n, n, batch)
+    ws = torch.empty(wb, dtype=torch.uint8, device=cuda)
+    L.call("euv_zgemm_tf32x3", n, n, n, L.c64.of(1.0), None, dA.data_ptr(), n, n * n,
+           dA.data_ptr(), n, n * n, L.c64.of(0), dC.data_ptr(), n, n * n, L.c64.of(0), batch,
+           steps.data_ptr(), 1, ws.data_ptr(), wb, _stream())
+    torch.cuda.synchronize()
+    got = _from_colmajor(dC.cpu().numpy(), n, n)
+    assert rel_err(got[0], A[0]) == 0.0
+    assert rel_err(got[1], A[1] @ A[1]) < 1e-5
+
+
+def test_matfun_mixed_close_to_fp64(cuda):
+    import torch
+    n = 300
+    rng = np.random.default_rng(5)
+    k = 2 * np.pi / 13.5
+    Dm = np.diag(k * k * (0.93 + 0.05j) - rng.uniform(0, 0.01, n)) + \
+        0.004 * (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))) / np.sqrt(n)
+    dD = _t(_colmajor(Dm[None]), cuda)
+    th = _t(np.array([60.0]), cuda)
+    out = {}
+    for prec in (L.EUV_PREC_FP64, L.EUV_PREC_MIXED):
+        dc, ds = torch.empty_like(dD), torch.empty_like(dD)
+        wb = L.lib().euv_matfun_workspace_bytes(n, 1)
+        ws = torch.empty(wb, dtype=torch.uint8, device=cuda)
+        L.call("euv_matfun_cs", n, dD.data_ptr(), th.data_ptr(), dc.data_ptr(), ds.data_ptr(), 1, 12,
+               prec, ws.data_ptr(), wb, _stream())
+        torch.cuda.synchronize()
+        out[prec] = (dc.cpu().numpy(), ds.cpu().numpy())
+    assert rel_err(out[L.EUV_PREC_MIXED][0], out[L.EUV_PREC_FP64][0]) < 1e-4
+    assert rel_err(out[L.EUV_PREC_MIXED][1], out[L.EUV_PREC_FP64][1]) < 1e-4

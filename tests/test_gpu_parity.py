@@ -123,3 +123,19 @@ def test_m3d_matches_oracle(cuda):
     if xin.any():
         assert rel_err(res["ax"][0].cpu().numpy()[xin], ref["ax"]) < 1e-7
         assert rel_err(res["ay"][0].cpu().numpy()[xin], ref["ay"]) < 1e-7
+
+
+@pytest.mark.parametrize("name", ["small", "mixed"])
+def test_mixed_precision_intensity_within_1e4(cuda, name):
+    """North-star bar of the mixed form: intensity within 1e-4 of the FP64 oracle."""
+    import torch
+    from euvlitho_b200.engine import Plan
+    cfg = preset(name)
+    oc = to_oracle(cfg)
+    plan = Plan(cfg, device=cuda, pols=("X", "Y"), precision="mixed")
+    ms = _masks(cfg, [31, 32])
+    img = plan.intensity(torch.from_numpy(np.stack([packed(m) for m in ms]))).cpu().numpy()
+    for c, m in enumerate(ms):
+        ref = O.intensity(oc, flat_bits(m), polars=("X", "Y"))
+        for p, pol in enumerate(("X", "Y")):
+            assert rel_err(img[c, p], ref[pol]) < 1e-4
