@@ -75,7 +75,7 @@ class AmpDesc(C.Structure):
         ("n_units", C.c_int),
         ("d_kx0", P), ("d_ky0", P), ("d_polar", P), ("d_spec", P),
         ("n_src", C.c_int), ("d_src_order", P), ("d_src_2kz", P),
-        ("precision", C.c_int), ("m_max", C.c_int),
+        ("precision", C.c_int), ("m_max", C.c_int), ("k0_max", C.c_double),
     ]
 
 

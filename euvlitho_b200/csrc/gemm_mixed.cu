@@ -6,7 +6,10 @@
 // lo = x - hi), and each real product is hi*hi + hi*lo + lo*hi with FP32
 // accumulation in tensor memory.  The complex product uses four real products:
 //   Re = ArBr - AiBi,  Im = ArBi + AiBr   (the minus sign through the MMA's
-//   negate-A bit), so one K step issues 12 tcgen05.mma into two accumulators.
+//   negate-A bit), so one K=8 step issues 12 tcgen05.mma into a Re and an Im
+//   accumulator.  The FP32 accumulation error grows with the K it spans, so
+//   the two halves of K have their own Re/Im accumulators (four in all),
+//   summed in FP64 by the epilogue.
 // Error per product ~1e-6 relative: the bulk products of the slab matrix
 // functions tolerate it (intensity error < 1e-4, see the tests); the interface
 // solves stay FP64.
@@ -14,10 +17,10 @@
 // Operands are first rewritten (split_*_kernel) as four fp32 planes
 // [batch][Re_hi, Re_lo, Im_hi, Im_lo][rows][Kp] with K contiguous (K-major for
 // both A and B), Kp = K rounded up to 16.  The GEMM kernel:
-//   warp 0     : TMA producer (3-D tensor maps, 64-byte swizzle, 2 stages of
-//                4x(128x16) A + 4x(256x16) B fp32 = 96 KB);
-//   warp 1     : TMEM allocation (512 columns: Re and Im accumulators of a
-//                128x256 tile) and the single-thread MMA issue loop;
+//   warp 0     : TMA producer (3-D tensor maps, 64-byte swizzle, 3 stages of
+//                4x(128x16) A + 4x(128x16) B fp32 = 64 KB);
+//   warp 1     : TMEM allocation (512 columns: four 128-column accumulators of
+//                a 128x128 tile) and the single-thread MMA issue loop;
 //   warps 2..5 : epilogue, tcgen05.ld of their 32 TMEM lanes (= rows), complex
 //                FP64 result written column by column (coalesced).
 // All waits are bounded (about 2 s); a timeout sets the error word, drains the
@@ -33,9 +36,9 @@ int zgemm(int m, int n, int k, cplx alpha, const double* scale, const double2* a
           cudaStream_t stream);
 
 constexpr int MX_BM = 128;
-constexpr int MX_BN = 256;
+constexpr int MX_BN = 128;
 constexpr int MX_BK = 16;  // fp32 elements: 64-byte rows, one 64B swizzle span
-constexpr int MX_STAGES = 2;
+constexpr int MX_STAGES = 3;
 constexpr int MX_PLANES = 4;
 constexpr int MX_A_TILE = MX_BM * MX_BK * 4;  // 8 KB
 constexpr int MX_B_TILE = MX_BN * MX_BK * 4;  // 16 KB
@@ -243,29 +246,36 @@ __global__ void __launch_bounds__(MX_THREADS, 1)
     }
   } else if (warp == 1) {
     if (lane == 0) {
-      // (A plane, B plane, negate A) for Re and Im; planes: 0 Re_hi 1 Re_lo 2 Im_hi 3 Im_lo
+      // Planes: 0 Re_hi 1 Re_lo 2 Im_hi 3 Im_lo.  The FP32 accumulation in
+      // TMEM loses precision in proportion to the K it runs over (measured: the
+      // error is the same for TF32-exact operands and grows linearly in K), so
+      // the K range is split in two halves with their own Re/Im accumulators,
+      // summed in FP64 by the epilogue.
+      // Products (A plane, B plane): Re = +ArBr -AiBi, Im = +ArBi +AiBr, each
+      // as hi*hi + hi*lo + lo*hi; the Re list's last three are negated.
       const int re_a[6] = {0, 0, 1, 2, 2, 3}, re_b[6] = {0, 1, 0, 2, 3, 2};
       const int im_a[6] = {0, 0, 1, 2, 2, 3}, im_b[6] = {2, 3, 2, 0, 1, 0};
       const uint32_t id_pos = idesc_tf32(false), id_neg = idesc_tf32(true);
-      const uint32_t t_re = tmem, t_im = tmem + (uint32_t)MX_BN;
+      const int half = (nkb + 1) / 2;  // k-blocks [0, half) -> set 0, [half, nkb) -> set 1
       for (int kb = 0; kb < nkb; ++kb) {
         const int s = kb % MX_STAGES;
         const uint32_t ph = (uint32_t)((kb / MX_STAGES) & 1);
         if (!mbar_wait(&full[s], ph, abort_flag, p.err)) break;
         tc_fence_after();
+        const int set = kb < half ? 0 : 1;
+        const uint32_t t_re = tmem + (uint32_t)(2 * set * MX_BN);
+        const uint32_t t_im = t_re + (uint32_t)MX_BN;
+        const int kb0 = set ? half : 0;
 #pragma unroll
         for (int k8 = 0; k8 < MX_BK / 8; ++k8) {
+          const uint32_t first = (kb != kb0 || k8) ? 1u : 0u;
 #pragma unroll
           for (int q = 0; q < 6; ++q) {
-            const uint64_t da = umma_desc_sw64(a_tile(s, re_a[q]) + k8 * 32);
-            const uint64_t db = umma_desc_sw64(b_tile(s, re_b[q]) + k8 * 32);
-            umma_tf32(t_re, da, db, q >= 3 ? id_neg : id_pos, (kb | k8 | q) ? 1u : 0u);
-          }
-#pragma unroll
-          for (int q = 0; q < 6; ++q) {
-            const uint64_t da = umma_desc_sw64(a_tile(s, im_a[q]) + k8 * 32);
-            const uint64_t db = umma_desc_sw64(b_tile(s, im_b[q]) + k8 * 32);
-            umma_tf32(t_im, da, db, id_pos, (kb | k8 | q) ? 1u : 0u);
+            umma_tf32(t_re, umma_desc_sw64(a_tile(s, re_a[q]) + k8 * 32),
+                      umma_desc_sw64(b_tile(s, re_b[q]) + k8 * 32), q >= 3 ? id_neg : id_pos,
+                      (first | q) ? 1u : 0u);
+            umma_tf32(t_im, umma_desc_sw64(a_tile(s, im_a[q]) + k8 * 32),
+                      umma_desc_sw64(b_tile(s, im_b[q]) + k8 * 32), id_pos, (first | q) ? 1u : 0u);
           }
         }
         umma_commit(&empty[s]);  // frees the stage when these MMAs complete
@@ -287,10 +297,12 @@ __global__ void __launch_bounds__(MX_THREADS, 1)
     if (ok) {
       for (int c0 = 0; c0 < MX_BN; c0 += 16) {
         if (n0 + c0 >= p.n) break;  // warp-uniform
-        uint32_t vr[16], vi[16];
+        uint32_t vr[16], vi[16], cr[16], ci[16];
         const uint32_t lane_addr = ((uint32_t)(q * 32) << 16);
         tmem_ld16(tmem + lane_addr + (uint32_t)c0, vr);
         tmem_ld16(tmem + lane_addr + (uint32_t)(MX_BN + c0), vi);
+        tmem_ld16(tmem + lane_addr + (uint32_t)(2 * MX_BN + c0), cr);
+        tmem_ld16(tmem + lane_addr + (uint32_t)(3 * MX_BN + c0), ci);
         tmem_ld_wait();
         if (row < p.m) {
 #pragma unroll
@@ -298,7 +310,11 @@ __global__ void __launch_bounds__(MX_THREADS, 1)
             const int col = n0 + c0 + j;
             if (col < p.n) {
               double2* cp = C + row + (long long)col * p.ldc;
-              cplx v = alpha * mk((double)__uint_as_float(vr[j]), (double)__uint_as_float(vi[j]));
+              // K halves: set 0 at columns [0, 2BN), set 1 (empty if nkb == 1) at [2BN, 4BN)
+              const double s1r = nkb > 1 ? (double)__uint_as_float(cr[j]) : 0.0;
+              const double s1i = nkb > 1 ? (double)__uint_as_float(ci[j]) : 0.0;
+              cplx v = alpha * mk((double)__uint_as_float(vr[j]) + s1r,
+                                  (double)__uint_as_float(vi[j]) + s1i);
               if (use_beta) {
                 double2 o = *cp;
                 v = v + beta * mk(o.x, o.y);
@@ -338,9 +354,10 @@ __device__ __forceinline__ void split_tf32(double x, float& hi, float& lo) {
 // A (col-major complex M x K) -> planes [b][4][M][Kp], K contiguous (transpose
 // through a 32x32 shared tile).
 __global__ void split_a_kernel(int M, int K, int Kp, const double2* A, long long lda,
-                               long long sa, float* out) {
+                               long long sa, float* out, const int* steps, int step) {
   __shared__ double2 tile[32][33];
   const int b = blockIdx.z;
+  if (steps != nullptr && step >= steps[b]) return;  // inactive entry: the GEMM copies
   const int m0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
   A += (long long)b * sa;
   const int tx = threadIdx.x, ty = threadIdx.y;
@@ -369,8 +386,9 @@ __global__ void split_a_kernel(int M, int K, int Kp, const double2* A, long long
 
 // B (col-major complex K x N) -> planes [b][4][N][Kp], K contiguous.
 __global__ void split_b_kernel(int K, int N, int Kp, const double2* B, long long ldb,
-                               long long sb, float* out) {
+                               long long sb, float* out, const int* steps, int step) {
   const int b = blockIdx.y;
+  if (steps != nullptr && step >= steps[b]) return;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long long)N * Kp) return;
   const int k = (int)(t % Kp), n = (int)(t / Kp);
@@ -463,10 +481,10 @@ int gemm_mixed(int m, int n, int k, cplx alpha, const double* scale, const doubl
   EUV_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int), stream));
   {
     dim3 g((m + 31) / 32, (kp + 31) / 32, batch), t(32, 8);
-    split_a_kernel<<<g, t, 0, stream>>>(m, k, kp, a, lda, sa, pa);
+    split_a_kernel<<<g, t, 0, stream>>>(m, k, kp, a, lda, sa, pa, steps, step);
     EUV_LAUNCH_CHECK();
     dim3 gb((unsigned)(((long long)n * kp + 255) / 256), batch);
-    split_b_kernel<<<gb, 256, 0, stream>>>(k, n, kp, b, ldb, sb, pb);
+    split_b_kernel<<<gb, 256, 0, stream>>>(k, n, kp, b, ldb, sb, pb, steps, step);
     EUV_LAUNCH_CHECK();
   }
   CUtensorMap ta, tb;

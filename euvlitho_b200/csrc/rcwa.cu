@@ -128,12 +128,36 @@ __global__ void build_dg_kernel(SliceParams p, const double2* spectra, const int
     cplx sig = p.sig_m1 * F;
     if (dc) sig.x += 1.0;
     const double kpi = pol == 0 ? kxi : kyi, kpj = pol == 0 ? kxj : kyj;
-    // G = i (k delta - kp_i/k sig kp_j)
-    cplx a = (-kpi / p.k * kpj) * sig;
-    if (i == j) a.x += p.k;
-    cplx v = cmul_i(a);
-    G[(long long)u * nn + t] = make_double2(v.x, v.y);
+    if (want_g == 2) {
+      // E = diag(kp/k) sigma diag(kp/k), with G = i k (I - E)
+      cplx v = (kpi / p.k * (kpj / p.k)) * sig;
+      G[(long long)u * nn + t] = make_double2(v.x, v.y);
+    } else {
+      // G = i (k delta - kp_i/k sig kp_j)
+      cplx a = (-kpi / p.k * kpj) * sig;
+      if (i == j) a.x += p.k;
+      cplx v = cmul_i(a);
+      G[(long long)u * nn + t] = make_double2(v.x, v.y);
+    }
   }
+}
+
+// Z = s * (R + E R) with R = diag(v) (dense == 0) or R dense: the first factor
+// of the Euler product (I - E)^-1 = (I + E)(I + E^2)(I + E^4)...
+__global__ void euler_first_diag_kernel(int n, cplx s, const double2* E, const double2* v,
+                                        double2* Z) {
+  const long long nn = (long long)n * n;
+  const int b = blockIdx.y;
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nn) return;
+  const long long o = (long long)b * nn + t;
+  const int i = (int)(t % n), j = (int)(t / n);
+  const double2 vv = v[(long long)b * n + j];
+  const double2 e = E[o];
+  cplx r = mk(e.x, e.y) * mk(vv.x, vv.y);
+  if (i == j) r = r + mk(vv.x, vv.y);
+  r = s * r;
+  Z[o] = make_double2(r.x, r.y);
 }
 
 // ---------------------------------------------------------------- multilayer
@@ -485,8 +509,9 @@ static int derive_m_max(const euv_amp_desc* d) {
   const double S = sqrt((double)lr2 * (double)mr2);
   const double twopi = 6.283185307179586476925286766559;
   // largest |kx|, |ky| over orders and families (family offsets < 2 pi/dx)
-  double kxm = twopi * (2 * d->lmax + 2) / d->dx + k;
-  double kym = twopi * (2 * d->mmax + 2) / d->dy + k;
+  const double k0 = d->k0_max > 0 ? d->k0_max : k;
+  double kxm = twopi * (2 * d->lmax + 2) / d->dx + k0;
+  double kym = twopi * (2 * d->mmax + 2) / d->dy + k0;
   int mm = 0;
   for (int n = 0; n < d->n_slices; ++n) {
     double er = d->eabs[n].re - 1.0, ei = d->eabs[n].im;
@@ -508,6 +533,32 @@ static int derive_m_max(const euv_amp_desc* d) {
     if (m > mm) mm = m;
   }
   return mm;
+}
+
+// Factors of the Euler product for (I - E)^-1, E = diag(kp/k) Sigma diag(kp/k).
+// A finite section of the Toeplitz operator of 1/eps(x) has 2-norm at most
+// sup |1/eps| = max(1, 1/|eps_abs|), so ||E||_2 <= (max|kp|/k)^2 max(1, 1/|eps|).
+// Returns the F with ||E||^(2^F) <= 1e-12, or 0 (use LU) when the bound is weak.
+static int euler_factors(const euv_amp_desc* d) {
+  const double twopi = 6.283185307179586476925286766559;
+  const double k0 = d->k0_max > 0 ? d->k0_max : d->k;
+  const double kpx = k0 + twopi * (d->lmax + 1) / d->dx;
+  const double kpy = k0 + twopi * (d->mmax + 1) / d->dy;
+  const double kp = kpx > kpy ? kpx : kpy;
+  double sup = 1.0;
+  for (int n = 0; n < d->n_slices; ++n) {
+    const double a = sqrt(d->eabs[n].re * d->eabs[n].re + d->eabs[n].im * d->eabs[n].im);
+    if (1.0 / a > sup) sup = 1.0 / a;
+  }
+  const double e = (kp / d->k) * (kp / d->k) * sup;
+  if (!(e < 0.5)) return 0;
+  int f = 1;
+  double v = e;  // ||E||^(2^f)
+  while (v > 1e-12 && f < 8) {
+    v = v * v;
+    ++f;
+  }
+  return f;
 }
 
 struct AmpLayout {
@@ -663,6 +714,33 @@ extern "C" int euv_amp(const euv_amp_desc* d, const euv_c64* d_spectra, euv_c64*
 
   const double2* spec = reinterpret_cast<const double2*>(d_spectra);
   MatfunBufs mb{w.P2, w.P3, w.P4, w.T1, w.W, w.norm, w.h, w.h2, w.h4, w.steps, w.capped};
+  // Mixed form: G^-1 by the Euler product (I - E)^-1 = prod_f (I + E^(2^f)),
+  // f < euler_f, when the config bound on ||E||_2 makes it converge fast.
+  const int euler_f = d->precision == EUV_PREC_MIXED ? euler_factors(d) : 0;
+  // factors f = 1..euler_f-1 applied to the partial product held in Zbuf (the
+  // f = 0 factor is applied by the caller); E^(2^f) ping-pongs between G and P2
+  auto euler_tail = [&](double2* Zbuf) -> int {
+    double2* P = w.G;
+    double2* Pn = w.P2;
+    double2* Zc = Zbuf;
+    double2* Zt = w.W;
+    for (int f = 1; f < euler_f; ++f) {
+      int r2 = gemm(N, N, N, one, nullptr, P, N, nn, P, N, nn, zero, Pn, N, nn, zero, U);
+      if (r2) return r2;
+      double2* t = P;
+      P = Pn;
+      Pn = t;
+      EUV_CUDA_TRY(cudaMemcpyAsync(Zt, Zc, (size_t)U * nn * sizeof(double2), cudaMemcpyDeviceToDevice, stream));
+      r2 = gemm(N, N, N, one, nullptr, P, N, nn, Zc, N, nn, one, Zt, N, nn, zero, U);
+      if (r2) return r2;
+      t = Zc;
+      Zc = Zt;
+      Zt = t;
+    }
+    if (Zc != Zbuf)
+      EUV_CUDA_TRY(cudaMemcpyAsync(Zbuf, Zc, (size_t)U * nn * sizeof(double2), cudaMemcpyDeviceToDevice, stream));
+    return EUV_OK;
+  };
   double2* X = w.X;
   double2* Y = w.Y;
   for (int n = NS - 1; n >= 0; --n) {
@@ -671,15 +749,36 @@ extern "C" int euv_amp(const euv_amp_desc* d, const euv_c64* d_spectra, euv_c64*
     const bool need_g = bottom || d->refresh_sigma;
     // bottom slice sigma is used for every slice unless refresh_sigma (header.h:1327-1353)
     build_dg_kernel<<<ge, bs, 0, stream>>>(q, spec, d->d_spec, d->d_lindex, d->d_mindex, d->d_kx0,
-                                           d->d_ky0, d->d_polar, w.D, w.G, 1, need_g ? 1 : 0);
+                                           d->d_ky0, d->d_polar, w.D, w.G, 1,
+                                           need_g ? (euler_f > 0 ? 2 : 1) : 0);
     EUV_LAUNCH_CHECK();
     double2* Zp = X;
-    if (bottom) {
+    if (bottom && euler_f > 0) {
+      // mixed form: Z = G^-1 diag(gx2) = (1/ik) (I - E)^-1 diag(gx2) by the Euler
+      // product on the tensor cores (E was built in place of G)
+      euler_first_diag_kernel<<<ge, bs, 0, stream>>>(N, cdiv(one, mk(0.0, d->k)), w.G, w.gx2, w.Z);
+      EUV_LAUNCH_CHECK();
+      if ((rc = euler_tail(w.Z))) return rc;
+      Zp = w.Z;
+    } else if (bottom) {
       // Z = G^-1 diag(Bru (URUU+URUB))
       diag_kernel<<<ge, bs, 0, stream>>>(N, w.gx2, w.Z);
       EUV_LAUNCH_CHECK();
       if ((rc = lu_factor(N, w.G, N, nn, w.ipiv, w.info, U, stream))) return rc;
       if ((rc = lu_solve(N, N, w.G, N, nn, w.ipiv, w.Z, N, nn, U, stream))) return rc;
+      Zp = w.Z;
+    } else if (d->refresh_sigma && euler_f > 0) {
+      // Z = (I - E_n)^-1 (I - E_{n+1}) X  (= G_n^-1 G_{n+1} X)
+      SliceParams qp = slice_params(n + 1);
+      build_dg_kernel<<<ge, bs, 0, stream>>>(qp, spec, d->d_spec, d->d_lindex, d->d_mindex,
+                                             d->d_kx0, d->d_ky0, d->d_polar, nullptr, w.Gp, 0, 2);
+      EUV_LAUNCH_CHECK();
+      EUV_CUDA_TRY(cudaMemcpyAsync(w.Z, X, (size_t)U * nn * sizeof(double2), cudaMemcpyDeviceToDevice, stream));
+      if ((rc = gemm(N, N, N, mk(-1.0, 0.0), nullptr, w.Gp, N, nn, X, N, nn, one, w.Z, N, nn, zero, U))) return rc;
+      EUV_CUDA_TRY(cudaMemcpyAsync(w.W, w.Z, (size_t)U * nn * sizeof(double2), cudaMemcpyDeviceToDevice, stream));
+      if ((rc = gemm(N, N, N, one, nullptr, w.G, N, nn, w.Z, N, nn, one, w.W, N, nn, zero, U))) return rc;
+      EUV_CUDA_TRY(cudaMemcpyAsync(w.Z, w.W, (size_t)U * nn * sizeof(double2), cudaMemcpyDeviceToDevice, stream));
+      if ((rc = euler_tail(w.Z))) return rc;
       Zp = w.Z;
     } else if (d->refresh_sigma) {
       // Z = G_n^-1 G_{n+1} X

@@ -186,6 +186,7 @@ class Plan:
         d.d_src_order, d.d_src_2kz = _ptr(src_order), _ptr(src_2kz)
         d.precision = self.precision
         d.m_max = 0
+        d.k0_max = float(max(kx0.abs().max().item(), ky0.abs().max().item()))
         keep.extend([t_l, t_m, kx0, ky0, polar, spec_of_unit, src_order, src_2kz])
         return d
 

@@ -120,6 +120,7 @@ typedef struct {
   const double* d_src_2kz; /* [U][n_src] 2*kz of each source (header.h:1401-1409) */
   int precision;         /* EUV_PREC_FP64 or EUV_PREC_MIXED */
   int m_max;             /* upper bound on double-angle steps; <= 0: derived */
+  double k0_max;         /* bound on |kx0|, |ky0| over the units (<= 0: k) */
 } euv_amp_desc;
 
 size_t euv_amp_workspace_bytes(const euv_amp_desc* desc);
