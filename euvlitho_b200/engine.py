@@ -378,7 +378,8 @@ class IntensityBatch:
     CUDA graph (``capture()`` / ``replay()``).  ``run_plain()`` is the
     unbatched FP64 form: one unit per ampS call."""
 
-    def __init__(self, plan: Plan, n_clips: int, n_mask_slices: int = 1):
+    def __init__(self, plan: Plan, n_clips: int, n_mask_slices: int = 1,
+                 max_units: Optional[int] = None, own_work: bool = True):
         cfg = plan.cfg
         self.plan = plan
         self.n_clips = nc = n_clips
@@ -426,60 +427,72 @@ class IntensityBatch:
         lib = L.lib()
         self.spec_bytes = lib.euv_mask_spectrum_workspace_bytes(nc * n_mask_slices, cfg.ndivx, cfg.ndivy,
                                                                cfg.fdivx, cfg.fdivy, self.lh, self.mh)
-        self.amp_bytes = lib.euv_amp_workspace_bytes(C.byref(self.desc))
+        self.max_units = U if max_units is None else max(1, min(int(max_units), U))
+        self.chunks = self._unit_descs(self.max_units)
+        self.amp_bytes = max(wb for _, _, _, wb in self.chunks)
         if self.amp_bytes == 0:
             raise ValueError("invalid ampS descriptor")
-        self.work = torch.empty(max(self.spec_bytes, self.amp_bytes), dtype=torch.uint8, device=dev)
+        self.work_bytes = max(self.spec_bytes, self.amp_bytes)
+        self.work = (torch.empty(self.work_bytes, dtype=torch.uint8, device=dev) if own_work
+                     else None)
         self.graph: Optional[torch.cuda.CUDAGraph] = None
         self._plain = None
 
-    def _spectra(self) -> None:
+    def _unit_descs(self, size: int):
+        """ampS / Abbe descriptors for units [u0, u0+size): pointer offsets into
+        the batch's per-unit tables (the C ABI takes plain pointers)."""
+        out = []
+        ns = self.ax.shape[1] * self.ax.shape[2]
+        nsrc = self.desc.n_src
+        for u0 in range(0, self.U, size):
+            n = min(size, self.U - u0)
+            d = L.AmpDesc.from_buffer_copy(self.desc)
+            d.n_units = n
+            d.d_kx0 = self.t_kx0.data_ptr() + 8 * u0
+            d.d_ky0 = self.t_ky0.data_ptr() + 8 * u0
+            d.d_polar = self.t_pol.data_ptr() + 4 * u0
+            d.d_spec = self.t_clip.data_ptr() + 4 * u0
+            d.d_src_order = self.t_order.data_ptr() + 4 * u0 * nsrc
+            d.d_src_2kz = self.t_kz2.data_ptr() + 8 * u0 * nsrc
+            a = L.AbbeDesc.from_buffer_copy(self.adesc)
+            a.n_units = n
+            a.d_tab_of_unit = self.t_tab.data_ptr() + 4 * u0
+            a.d_img_of_unit = self.t_img.data_ptr() + 4 * u0
+            a.d_nsrc_of_unit = self.t_ns.data_ptr() + 4 * u0
+            wb = L.lib().euv_amp_workspace_bytes(C.byref(d))
+            out.append((d, a, self.ax.data_ptr() + 16 * ns * u0, wb))
+        return out
+
+    def _spectra(self, work: torch.Tensor) -> None:
         cfg = self.plan.cfg
         n = self.masks.shape[0] * self.masks.shape[1]
         L.call("euv_mask_spectrum", self.masks.data_ptr(), n, cfg.ndivx, cfg.ndivy, cfg.fdivx,
                cfg.fdivy, self.lh, self.mh, 0, cfg.yflip_offset, self.spec_raw.data_ptr(),
-               self.work.data_ptr(), self.work.numel(), _stream())
+               work.data_ptr(), work.numel(), _stream())
         if self.spec.data_ptr() != self.spec_raw.data_ptr():
             self.spec.copy_(self.spec_raw.view(self.n_clips, 1, -1).expand_as(self.spec))
 
-    def run(self) -> None:
-        self._spectra()
-        L.call("euv_amp", C.byref(self.desc), self.spec.data_ptr(), self.ax.data_ptr(),
-               self.work.data_ptr(), self.work.numel(), _stream())
+    def run(self, work: Optional[torch.Tensor] = None) -> None:
+        """Enqueue spectra, batched ampS (in chunks of max_units units sharing
+        one workspace) and the fused Abbe kernel on the current stream.
+        ``work``: a workspace of at least ``work_bytes`` (default: the batch's own)."""
+        w = self.work if work is None else work
+        self._spectra(w)
+        for d, _, axp, _ in self.chunks:
+            L.call("euv_amp", C.byref(d), self.spec.data_ptr(), axp, w.data_ptr(), w.numel(),
+                   _stream())
         self.image.zero_()
         L.call("euv_abbe", C.byref(self.adesc), self.ax.data_ptr(), self.image.data_ptr(), _stream())
 
-    def _plain_descs(self):
-        if self._plain is not None:
-            return self._plain
-        descs = []
-        ns = self.ax.shape[1] * self.ax.shape[2]
-        for u in range(self.U):
-            d = L.AmpDesc.from_buffer_copy(self.desc)
-            d.n_units = 1
-            d.d_kx0 = self.t_kx0.data_ptr() + 8 * u
-            d.d_ky0 = self.t_ky0.data_ptr() + 8 * u
-            d.d_polar = self.t_pol.data_ptr() + 4 * u
-            d.d_spec = self.t_clip.data_ptr() + 4 * u
-            d.d_src_order = self.t_order.data_ptr() + 4 * u * self.desc.n_src
-            d.d_src_2kz = self.t_kz2.data_ptr() + 8 * u * self.desc.n_src
-            a = L.AbbeDesc.from_buffer_copy(self.adesc)
-            a.n_units = 1
-            a.d_tab_of_unit = self.t_tab.data_ptr() + 4 * u
-            a.d_img_of_unit = self.t_img.data_ptr() + 4 * u
-            a.d_nsrc_of_unit = self.t_ns.data_ptr() + 4 * u
-            descs.append((d, a, self.ax.data_ptr() + 16 * ns * u))
-        wb = L.lib().euv_amp_workspace_bytes(C.byref(descs[0][0]))
-        self._plain = (descs, wb)
-        return self._plain
-
-    def run_plain(self) -> None:
+    def run_plain(self, work: Optional[torch.Tensor] = None) -> None:
         """The unbatched FP64 form: every unit solved and imaged on its own."""
-        descs, wb = self._plain_descs()
-        self._spectra()
+        if self._plain is None:
+            self._plain = self._unit_descs(1)
+        w = self.work if work is None else work
+        self._spectra(w)
         self.image.zero_()
-        for d, a, axp in descs:
-            L.call("euv_amp", C.byref(d), self.spec.data_ptr(), axp, self.work.data_ptr(), wb, _stream())
+        for d, a, axp, wb in self._plain:
+            L.call("euv_amp", C.byref(d), self.spec.data_ptr(), axp, w.data_ptr(), wb, _stream())
             L.call("euv_abbe", C.byref(a), axp, self.image.data_ptr(), _stream())
 
     def capture(self) -> None:

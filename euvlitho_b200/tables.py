@@ -190,6 +190,28 @@ def abbe_table(cfg: SimConfig, pol: str, ndivs: int, fam: Family, pos, linput, m
     return coef, nidx
 
 
+def required_orders(cfg: SimConfig) -> Tuple[int, int]:
+    """Largest |l|, |m| of the diffracted orders the Abbe loop reads: source
+    order + pupil order inside the pupil NA (intensity.cpp:320-321, 356).  An
+    order set must contain them (the reference reads its -1000 sentinel
+    otherwise, intensity.cpp:297-299)."""
+    k, dx, dy, MX, MY, NA = cfg.k, cfg.dx, cfg.dy, cfg.mx, cfg.my, cfg.na
+    ndivs, fams = sources(cfg)
+    lin, mn, _, _ = pupil_set(cfg)
+    lmax = mmax = 0
+    for f in fams:
+        pts = np.array(f.pts)
+        l0 = pts[:, 0][:, None]
+        m0 = pts[:, 1][:, None]
+        kxn = 2.0 * PI / dx * f.nsx / float(ndivs) + 2.0 * PI / dx * l0 + 2.0 * PI * lin[None, :] / dx
+        kyn = 2.0 * PI / dy * f.nsy / float(ndivs) + 2.0 * PI / dy * m0 + 2.0 * PI * mn[None, :] / dy
+        ok = (MX * MX * kxn * kxn + MY * MY * kyn * kyn) <= (NA * k) ** 2
+        if ok.any():
+            lmax = max(lmax, int(np.abs(l0 + lin[None, :])[ok].max()))
+            mmax = max(mmax, int(np.abs(m0 + mn[None, :])[ok].max()))
+    return lmax, mmax
+
+
 def row_starts(linput: np.ndarray, lpx: int) -> np.ndarray:
     """row_start[l] = first pupil point with linput = l - lpx (points are l-major)."""
     if np.any(np.diff(linput) < 0):

@@ -1,0 +1,41 @@
+"""Serving: continuous batching returns, for every request, the image the same
+clip gets when it is computed alone (CPU checks of the workload generator, GPU
+check of the results)."""
+import numpy as np
+import pytest
+
+from euvlitho_b200 import serving as S
+
+
+def test_workload_is_poisson_and_propagating():
+    reqs = S.workload(400, rate=50.0, seed=3)
+    t = np.array([r.arrival for r in reqs])
+    gaps = np.diff(np.r_[0.0, t])
+    assert abs(gaps.mean() - 1 / 50.0) < 0.2 / 50.0          # mean rate
+    assert all(S.propagating(r.key.period, r.key.box) for r in reqs)
+    assert {r.key.period for r in reqs} == set(S.PERIODS)
+    assert {r.key.n_src for r in reqs} <= set(S.SOURCE_COUNTS)
+
+
+def test_config_for_gives_the_requested_source_count():
+    from euvlitho_b200 import tables as T
+    for key in (S.ClipKey(256, 5, 50), S.ClipKey(1024, 15, 200), S.ClipKey(512, 10, 100)):
+        cfg = S.config_for(key)
+        n = sum(len(f.pts) for f in T.sources(cfg)[1])
+        assert n == key.n_src
+        assert (cfg.ndivx, cfg.lbox) == (key.period, key.box)
+
+
+@pytest.mark.gpu
+def test_each_result_same_alone_and_in_the_mix(cuda):
+    import torch
+    reqs = S.workload(24, rate=400.0, seed=5, periods=(256, 512), boxes=(5,), source_counts=(50,))
+    srv = S.Server(device=cuda, precision="mixed", max_batch=4, n_streams=3)
+    srv.warm(sorted({r.key for r in reqs}, key=lambda k: (k.period, k.box, k.n_src)))
+    stats = srv.serve(reqs)
+    assert stats["requests"] == len(reqs) and stats["mean_batch"] > 1.0
+    for r in reqs:
+        plan = srv.plan(r.key)
+        alone = plan.intensity(torch.from_numpy(r.mask[None])).cpu().numpy()[0]
+        err = np.max(np.abs(r.image - alone)) / np.max(np.abs(alone))
+        assert err < 1e-12, (r.rid, err)
