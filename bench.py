@@ -111,6 +111,28 @@ def run_reference(a) -> int:
     return 0
 
 
+# ---------------------------------------------------------------- ranks
+def rank_seeds(rank: int, clips: int):
+    """Each rank images its own clips (replicas: disjoint seeded masks)."""
+    return [1000 * rank + i for i in range(clips)]
+
+
+def max_over_ranks_on(x: float, world: int, device) -> float:
+    """Max of a per-rank timing over all ranks (the slowest rank sets the time)."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(clips_per_rank: int, world: int, max_ms_per_step: float) -> float:
+    """Clips/s of the whole job: every rank's clips over the slowest rank's time."""
+    return clips_per_rank * world / (max_ms_per_step / 1000.0)
+
+
 # ---------------------------------------------------------------- clocks
 class Clocks:
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -182,15 +204,11 @@ def main() -> int:
             dist.barrier()
 
     def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return max_over_ranks_on(x, world, dev)
 
     cfg = preset("batched")
     plan = Plan(cfg, device=dev, pols=("X", "Y"), precision=a.precision)
-    host = MK.batch(cfg.ndivx, cfg.ndivy, [1000 * rank + i for i in range(CLIPS)])
+    host = MK.batch(cfg.ndivx, cfg.ndivy, rank_seeds(rank, CLIPS))
     b = plan.intensity_batch(CLIPS)
     b.masks.copy_(torch.from_numpy(host))
     lib = L.lib()
@@ -220,7 +238,7 @@ def main() -> int:
     step_ms = [ev[i].elapsed_time(ev[i + 1]) for i in range(a.steps)]
     total_ms = max_over_ranks(ev[0].elapsed_time(ev[-1]))
     ms_per_step = total_ms / a.steps
-    value = CLIPS * world / (total_ms / 1000.0 / a.steps)
+    value = whole_job_rate(CLIPS, world, total_ms / a.steps)
     lat = sorted(step_ms)
     p50 = lat[len(lat) // 2]
     p99 = lat[min(len(lat) - 1, int(round(0.99 * (len(lat) - 1))))]
