@@ -133,6 +133,86 @@ def whole_job_rate(clips_per_rank: int, world: int, max_ms_per_step: float) -> f
     return clips_per_rank * world / (max_ms_per_step / 1000.0)
 
 
+# ---------------------------------------------------------------- roofline
+def _time_ms(fn, stream, reps):
+    import torch
+    fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def _traffic(name: str):
+    """DRAM bytes per launch of the kernel at the bench shape, from the ncu
+    summary committed under profiles/ (None if absent)."""
+    tp = os.path.join(ROOT, "profiles", name)
+    try:
+        return json.load(open(tp)).get("dram_bytes_per_launch_at_bench_shape")
+    except (OSError, ValueError):
+        return None
+
+
+def dominant_kernel_roofline(plan, U, precision, dev, stream, L):
+    """Roofline of the step's dominant kernel at the pipeline's shape (all U
+    units of N orders), timed live with CUDA events on the launching stream.
+
+    mixed: the tcgen05 TF32x3 complex GEMM; algorithmic work = 24*N^3 TF32
+    FLOP per unit (3 split products x 4 real products x 2N^3), peak = cuBLAS
+    TF32 GEMM measured in this run.  fp64: the DMMA complex GEMM, 8*N^3 FLOP
+    per unit, peak = cuBLAS ZGEMM measured in this run.  (MEASURED_PEAKS.json
+    holds BF16 and HBM peaks only.)"""
+    import torch
+    N = plan.orders.n
+    A = torch.randn(U, N, N, dtype=torch.complex128, device=dev)
+    B = torch.randn(U, N, N, dtype=torch.complex128, device=dev)
+    C = torch.empty_like(A)
+    s = stream.cuda_stream
+    if precision == "mixed":
+        wb = L.lib().euv_zgemm_tf32x3_workspace_bytes(N, N, N, U)
+        ws = torch.empty(wb, dtype=torch.uint8, device=dev)
+
+        def gemm():
+            L.call("euv_zgemm_tf32x3", N, N, N, L.c64(1, 0), None, A.data_ptr(), N, N * N,
+                   B.data_ptr(), N, N * N, L.c64(0, 0), C.data_ptr(), N, N * N, L.c64(0, 0), U,
+                   None, 0, ws.data_ptr(), wb, s)
+        flop = 24.0 * N ** 3 * U
+        ms = _time_ms(gemm, stream, 5)
+        X = torch.randn(8192, 8192, dtype=torch.float32, device=dev)
+        Y = torch.randn(8192, 8192, dtype=torch.float32, device=dev)
+        old = torch.backends.cuda.matmul.allow_tf32
+        torch.backends.cuda.matmul.allow_tf32 = True
+        peak = 2.0 * 8192 ** 3 / (_time_ms(lambda: torch.matmul(X, Y), stream, 5) / 1e3) / 1e12
+        torch.backends.cuda.matmul.allow_tf32 = old
+        out = {"bound": "tensor",
+               "kernel": "gemm_tf32x3_kernel (tcgen05 kind::tf32, TMA, TMEM) incl. operand split, "
+                         "batch %d x %d^3 complex" % (U, N),
+               "peak_source": "cuBLAS TF32 GEMM 8192^3 (torch.matmul float32, allow_tf32) measured "
+                              "in this run",
+               "complex_fp64_equivalent_tflops": 8.0 * N ** 3 * U / (ms / 1e3) / 1e12,
+               "traffic": _traffic("gemm_tf32x3_n961.json")}
+    else:
+        def gemm():
+            L.call("euv_zgemm", N, N, N, L.c64(1, 0), None, A.data_ptr(), N, N * N, B.data_ptr(),
+                   N, N * N, L.c64(0, 0), C.data_ptr(), N, N * N, L.c64(0, 0), U, None, 0, s)
+        flop = 8.0 * N ** 3 * U
+        ms = _time_ms(gemm, stream, 5)
+        X = torch.randn(4096, 4096, dtype=torch.complex128, device=dev)
+        Y = torch.randn(4096, 4096, dtype=torch.complex128, device=dev)
+        peak = 8.0 * 4096 ** 3 / (_time_ms(lambda: torch.matmul(X, Y), stream, 3) / 1e3) / 1e12
+        out = {"bound": "tensor", "kernel": "zgemm_kernel (DMMA m8n8k4 f64), batch %d x %d^3" % (U, N),
+               "peak_source": "cuBLAS ZGEMM 4096^3 (torch.matmul complex128) measured in this run",
+               "traffic": _traffic("zgemm_n961.json")}
+    achieved = flop / (ms / 1e3) / 1e12
+    out.update({"achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "ms_per_launch": ms, "algorithmic_flop_per_launch": flop})
+    return out
+
+
 # ---------------------------------------------------------------- clocks
 class Clocks:
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -281,54 +361,7 @@ def main() -> int:
     plain_ms = max_over_ranks(p0.elapsed_time(p1))
     plain_value = CLIPS * world / (plain_ms / 1000.0)
 
-    # ---- roofline of the dominant kernel: the batched complex FP64 GEMM at
-    # the pipeline's shape (N=961, all 24 units), timed live with CUDA events
-    N, U = plan.orders.n, b.U
-    A = torch.randn(U, N, N, dtype=torch.complex128, device=dev)
-    Bm = torch.randn(U, N, N, dtype=torch.complex128, device=dev)
-    Cm = torch.empty_like(A)
-    reps = 5
-
-    def zg():
-        L.call("euv_zgemm", N, N, N, L.c64(1, 0), None, A.data_ptr(), N, N * N, Bm.data_ptr(), N,
-               N * N, L.c64(0, 0), Cm.data_ptr(), N, N * N, L.c64(0, 0), U, None, 0,
-               stream.cuda_stream)
-    zg()
-    torch.cuda.synchronize()
-    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    g0.record(stream)
-    for _ in range(reps):
-        zg()
-    g1.record(stream)
-    torch.cuda.synchronize()
-    zg_ms = g0.elapsed_time(g1) / reps
-    zg_tflops = 8.0 * N ** 3 * U / (zg_ms / 1000.0) / 1e12
-    # FP64 tensor reference: cuBLAS ZGEMM (torch.matmul complex128), 4096^3
-    X = torch.randn(4096, 4096, dtype=torch.complex128, device=dev)
-    Y = torch.randn(4096, 4096, dtype=torch.complex128, device=dev)
-    torch.matmul(X, Y)
-    torch.cuda.synchronize()
-    c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    c0.record(stream)
-    for _ in range(3):
-        torch.matmul(X, Y)
-    c1.record(stream)
-    torch.cuda.synchronize()
-    cublas_tflops = 8.0 * 4096 ** 3 / (c0.elapsed_time(c1) / 3 / 1000.0) / 1e12
-    del A, Bm, Cm, X, Y
-    traffic = None
-    tp = os.path.join(ROOT, "profiles", "zgemm_batched_n961_traffic.json")
-    if os.path.exists(tp):
-        try:
-            traffic = json.load(open(tp)).get("dram_bytes_per_launch")
-        except (OSError, ValueError):
-            traffic = None
-    roofline = {"bound": "tensor", "kernel": "zgemm_kernel (DMMA m8n8k4 f64), batch 24 x 961^3",
-                "achieved": zg_tflops, "peak": cublas_tflops, "unit": "TFLOP/s",
-                "frac": zg_tflops / cublas_tflops, "traffic": traffic,
-                "peak_source": "cuBLAS ZGEMM 4096^3 (torch.matmul complex128) measured in this run; "
-                               "the bf16/HBM peaks of MEASURED_PEAKS.json do not apply to FP64",
-                "algorithmic_flop_per_launch": 8.0 * N ** 3 * U}
+    roofline = dominant_kernel_roofline(plan, b.U, a.precision, dev, stream, L)
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -344,7 +377,7 @@ def main() -> int:
         "dtype": "f64" if a.precision == "fp64" else "tf32x3+f64",
         "data": "synthetic (seeded lines+contacts masks, 36% absorber)",
         "config": {"workload": WORKLOAD, "clips_per_step": CLIPS, "precision": a.precision,
-                   "units_per_step": b.U, "orders": N,
+                   "units_per_step": b.U, "orders": plan.orders.n,
                    "l2": "working set %.1f GB per step > 126 MB L2 (no flush needed)"
                          % (b.work.numel() / 1e9),
                    "parallelism": "replicas x%d" % world, "cuda_graph": True},

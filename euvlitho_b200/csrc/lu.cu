@@ -115,6 +115,179 @@ __global__ void __launch_bounds__(LU_PANEL_THREADS) lu_panel_kernel(int n, int j
   }
 }
 
+// Panel factorisation with register-resident sub-panels (N <= 512*RPT): the
+// panel is factored LP_SB columns at a time; thread t holds rows
+// r0 + t + k*LP_THREADS (k < RPT) of the sub-panel in registers, so pivot
+// search, row exchange, scaling and the rank-1 updates inside the sub-panel
+// touch no global memory.  After each sub-panel, the rest of the panel is
+// brought up to date at once (U12 = L11^-1 A12, A22 -= L21 U12): one global
+// read-modify-write per sub-panel instead of one per column.
+constexpr int LP_THREADS = 512;
+constexpr int LP_SB = 4;
+
+template <int RPT>
+__global__ void __launch_bounds__(LP_THREADS) lu_panel_reg_kernel(int n, int j0, int jb,
+                                                                  double2* A, long long lda,
+                                                                  long long sa, int* ipiv,
+                                                                  int* info) {
+  A += (long long)blockIdx.x * sa;
+  ipiv += (long long)blockIdx.x * n;
+  __shared__ double red_v[LP_THREADS / 32];
+  __shared__ int red_i[LP_THREADS / 32];
+  __shared__ int s_piv;
+  __shared__ cplx s_rowa[LP_SB], s_rowb[LP_SB], s_prow[LP_SB];
+  __shared__ cplx s_u12[LP_SB][LU_NB];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int sub = 0; sub < jb; sub += LP_SB) {
+    const int sb = (jb - sub) < LP_SB ? (jb - sub) : LP_SB;
+    const int c0 = j0 + sub;
+    cplx v[RPT][LP_SB];
+#pragma unroll
+    for (int k = 0; k < RPT; ++k) {
+      const int r = c0 + tid + k * LP_THREADS;
+#pragma unroll
+      for (int c = 0; c < LP_SB; ++c)
+        v[k][c] = (r < n && c < sb) ? ld2(&A[r + (long long)(c0 + c) * lda]) : mk(0.0, 0.0);
+    }
+    for (int c = 0; c < sb; ++c) {
+      const int jj = c0 + c;
+      // pivot: first index of max |re|+|im| in rows jj..n-1 (LAPACK izamax)
+      double best = -1.0;
+      int bidx = n;
+#pragma unroll
+      for (int k = 0; k < RPT; ++k) {
+        const int r = c0 + tid + k * LP_THREADS;
+        if (r >= jj && r < n) {
+          const double a = cabs1(v[k][c]);
+          if (a > best) {
+            best = a;
+            bidx = r;
+          }
+        }
+      }
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        const double ov = __shfl_down_sync(0xffffffffu, best, off);
+        const int oi = __shfl_down_sync(0xffffffffu, bidx, off);
+        if (ov > best || (ov == best && oi < bidx)) {
+          best = ov;
+          bidx = oi;
+        }
+      }
+      if (lane == 0) {
+        red_v[warp] = best;
+        red_i[warp] = bidx;
+      }
+      __syncthreads();
+      if (tid == 0) {
+        double bv = red_v[0];
+        int bi = red_i[0];
+        for (int w = 1; w < LP_THREADS / 32; ++w)
+          if (red_v[w] > bv || (red_v[w] == bv && red_i[w] < bi)) {
+            bv = red_v[w];
+            bi = red_i[w];
+          }
+        if (bi >= n) bi = jj;
+        s_piv = bi;
+        ipiv[jj] = bi;
+      }
+      __syncthreads();
+      const int piv = s_piv;
+      if (piv != jj) {
+#pragma unroll
+        for (int k = 0; k < RPT; ++k) {
+          const int r = c0 + tid + k * LP_THREADS;
+#pragma unroll
+          for (int cc = 0; cc < LP_SB; ++cc) {
+            if (r == jj) s_rowa[cc] = v[k][cc];
+            if (r == piv) s_rowb[cc] = v[k][cc];
+          }
+        }
+        // the panel's other columns: exchange rows jj and piv in global memory
+        for (int t = tid; t < jb - sb; t += LP_THREADS) {
+          const int col = t < sub ? j0 + t : j0 + t + sb;
+          double2 x = A[jj + (long long)col * lda];
+          A[jj + (long long)col * lda] = A[piv + (long long)col * lda];
+          A[piv + (long long)col * lda] = x;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < RPT; ++k) {
+          const int r = c0 + tid + k * LP_THREADS;
+#pragma unroll
+          for (int cc = 0; cc < LP_SB; ++cc) {
+            if (r == jj) v[k][cc] = s_rowb[cc];
+            if (r == piv) v[k][cc] = s_rowa[cc];
+          }
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < RPT; ++k) {
+        const int r = c0 + tid + k * LP_THREADS;
+        if (r == jj)
+#pragma unroll
+          for (int cc = 0; cc < LP_SB; ++cc) s_prow[cc] = v[k][cc];
+      }
+      __syncthreads();
+      const cplx d = s_prow[c];
+      if (d.x == 0.0 && d.y == 0.0) {
+        if (tid == 0 && info[blockIdx.x] == 0) info[blockIdx.x] = jj + 1;
+        continue;
+      }
+      const cplx inv = cdiv(mk(1.0, 0.0), d);
+#pragma unroll
+      for (int k = 0; k < RPT; ++k) {
+        const int r = c0 + tid + k * LP_THREADS;
+        if (r > jj && r < n) {
+          v[k][c] = v[k][c] * inv;
+#pragma unroll
+          for (int cc = 0; cc < LP_SB; ++cc)
+            if (cc > c && cc < sb) v[k][cc] = v[k][cc] - v[k][c] * s_prow[cc];
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < RPT; ++k) {
+      const int r = c0 + tid + k * LP_THREADS;
+      if (r < n)
+#pragma unroll
+        for (int c = 0; c < LP_SB; ++c)
+          if (c < sb) st2(&A[r + (long long)(c0 + c) * lda], v[k][c]);
+    }
+    const int rest = j0 + jb - (c0 + sb);  // panel columns right of the sub-panel
+    if (rest > 0) {
+      __syncthreads();
+      // U12 = L11^-1 A12 (unit lower L11 = sub-panel rows c0..c0+sb-1)
+      if (tid < rest) {
+        const int col = c0 + sb + tid;
+        for (int i = 0; i < sb; ++i) {
+          cplx u = ld2(&A[c0 + i + (long long)col * lda]);
+          for (int q = 0; q < i; ++q) u = u - ld2(&A[c0 + i + (long long)(c0 + q) * lda]) * s_u12[q][tid];
+          s_u12[i][tid] = u;
+          st2(&A[c0 + i + (long long)col * lda], u);
+        }
+      }
+      __syncthreads();
+      // A22 -= L21 U12 for rows below the sub-panel (L21 in registers)
+#pragma unroll
+      for (int k = 0; k < RPT; ++k) {
+        const int r = c0 + tid + k * LP_THREADS;
+        if (r >= c0 + sb && r < n) {
+          for (int j = 0; j < rest; ++j) {
+            double2* p = &A[r + (long long)(c0 + sb + j) * lda];
+            cplx acc = ld2(p);
+#pragma unroll
+            for (int q = 0; q < LP_SB; ++q)
+              if (q < sb) acc = acc - v[k][q] * s_u12[q][j];
+            st2(p, acc);
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // Row swaps ipiv[j0..j0+jb) applied to every column outside [skip0, skip1).
 __global__ void lu_laswp_kernel(int n, int ncols, int j0, int jb, int skip0, int skip1,
                                 double2* A, long long lda, long long sa, const int* ipiv,
@@ -195,7 +368,14 @@ int lu_factor(int n, double2* A, long long lda, long long sa, int* ipiv, int* in
   EUV_LAUNCH_CHECK();
   for (int j0 = 0; j0 < n; j0 += LU_NB) {
     const int jb = (n - j0) < LU_NB ? (n - j0) : LU_NB;
-    lu_panel_kernel<<<batch, LU_PANEL_THREADS, 0, stream>>>(n, j0, jb, A, lda, sa, ipiv, info);
+    if (n <= LP_THREADS)
+      lu_panel_reg_kernel<1><<<batch, LP_THREADS, 0, stream>>>(n, j0, jb, A, lda, sa, ipiv, info);
+    else if (n <= 2 * LP_THREADS)
+      lu_panel_reg_kernel<2><<<batch, LP_THREADS, 0, stream>>>(n, j0, jb, A, lda, sa, ipiv, info);
+    else if (n <= 4 * LP_THREADS)
+      lu_panel_reg_kernel<4><<<batch, LP_THREADS, 0, stream>>>(n, j0, jb, A, lda, sa, ipiv, info);
+    else
+      lu_panel_kernel<<<batch, LU_PANEL_THREADS, 0, stream>>>(n, j0, jb, A, lda, sa, ipiv, info);
     EUV_LAUNCH_CHECK();
     dim3 gs((n + 127) / 128, batch);
     lu_laswp_kernel<<<gs, 128, 0, stream>>>(n, n, j0, jb, j0, j0 + jb, A, lda, sa, ipiv, n);

@@ -1,0 +1,157 @@
+"""Kernel microbenchmarks at the shapes of the measured workloads.
+
+  python -m euvlitho_b200.microbench tf32x3 --n 961 --batch 4
+  python -m euvlitho_b200.microbench zgemm  --n 961 --batch 4
+  python -m euvlitho_b200.microbench lu     --n 961 --batch 24 --nrhs 96
+  python -m euvlitho_b200.microbench step   --precision mixed --clips 4
+  python -m euvlitho_b200.microbench summarize launches.csv
+
+Times each library entry point with CUDA events on the launching stream after
+warm-up and prints one JSON line (the commands the ncu summaries in profiles/
+are taken from).  `step` runs one pipeline step of the batched workload
+(1024 nm box, 15 Bloch units per clip and polarisation pair) untimed, then
+`--reps` steps between cudaProfilerStart/Stop, so that
+`ncu --profile-from-start off` lists exactly those steps' launches.
+`summarize` folds an ncu `--csv` launch list of gpu__time_duration.sum into
+launches, total time and share per kernel.
+"""
+from __future__ import annotations
+
+import argparse
+import collections
+import csv
+import json
+import sys
+
+import torch
+
+from . import _lib as L
+
+
+def summarize(path: str) -> str:
+    hdr, agg = None, collections.defaultdict(lambda: [0, 0.0])
+    for r in csv.reader(open(path)):
+        if r and r[0] == "ID":
+            hdr = r
+            continue
+        if not hdr or len(r) != len(hdr):
+            continue
+        d = dict(zip(hdr, r))
+        if d.get("Metric Name") != "gpu__time_duration.sum":
+            continue
+        v = float(d["Metric Value"].replace(",", ""))
+        u = d["Metric Unit"]
+        v = v / 1e3 if u in ("ns", "nsecond") else (v * 1e3 if u in ("ms", "msecond") else v)
+        k = d["Kernel Name"].split("(")[0].replace("euv::", "")
+        if k.startswith("void at::"):
+            k = "torch " + k[len("void at::"):].split("<")[0]
+        agg[k][0] += 1
+        agg[k][1] += v
+    tot = sum(v[1] for v in agg.values()) or 1.0
+    lines = ["| kernel | launches | total us | share |", "|---|---:|---:|---:|"]
+    for k, v in sorted(agg.items(), key=lambda x: -x[1][1]):
+        lines.append("| %s | %d | %.1f | %.1f%% |" % (k, v[0], v[1], 100 * v[1] / tot))
+    lines.append("| total | %d | %.1f | 100%% |" % (sum(v[0] for v in agg.values()), tot))
+    return "\n".join(lines)
+
+
+def _step(a) -> dict:
+    from . import masks as MK
+    from .config import preset
+    from .engine import Plan
+    cfg = preset(a.preset)
+    plan = Plan(cfg, device=torch.device("cuda"), pols=("X", "Y"), precision=a.precision)
+    b = plan.intensity_batch(a.clips)
+    b.masks.copy_(torch.from_numpy(MK.batch(cfg.ndivx, cfg.ndivy, range(a.clips))))
+    b.run()
+    torch.cuda.synchronize()
+    n0 = L.lib().euv_kernel_launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.profiler.start()
+    e0.record()
+    for _ in range(a.reps):
+        b.run()
+    e1.record()
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    return {"preset": a.preset, "precision": a.precision, "clips": a.clips, "units": b.U,
+            "ms_per_step": e0.elapsed_time(e1) / a.reps,
+            "launches_per_step": (L.lib().euv_kernel_launches() - n0) // a.reps}
+
+
+def _time(fn, reps: int) -> float:
+    for _ in range(3):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("kernel", choices=["tf32x3", "zgemm", "lu", "step", "summarize"])
+    ap.add_argument("csv", nargs="?", help="ncu --csv launch list (summarize)")
+    ap.add_argument("--n", type=int, default=961)
+    ap.add_argument("--batch", type=int, default=4)
+    ap.add_argument("--nrhs", type=int, default=96)
+    ap.add_argument("--reps", type=int, default=10)
+    ap.add_argument("--preset", default="batched")
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--clips", type=int, default=4)
+    a = ap.parse_args(argv)
+    if a.kernel == "summarize":
+        print(summarize(a.csv))
+        return 0
+    if a.kernel == "step":
+        print(json.dumps(_step(a)))
+        return 0
+    n, b = a.n, a.batch
+    s = torch.cuda.current_stream().cuda_stream
+    g = torch.Generator(device="cuda").manual_seed(0)
+    A = torch.randn(b, n, n, dtype=torch.complex128, device="cuda", generator=g)
+    out = {"kernel": a.kernel, "n": n, "batch": b}
+    if a.kernel in ("tf32x3", "zgemm"):
+        B = torch.randn(b, n, n, dtype=torch.complex128, device="cuda", generator=g)
+        C = torch.empty_like(A)
+        if a.kernel == "tf32x3":
+            wb = L.lib().euv_zgemm_tf32x3_workspace_bytes(n, n, n, b)
+            ws = torch.empty(wb, dtype=torch.uint8, device="cuda")
+
+            def fn():
+                L.call("euv_zgemm_tf32x3", n, n, n, L.c64(1, 0), None, A.data_ptr(), n, n * n,
+                       B.data_ptr(), n, n * n, L.c64(0, 0), C.data_ptr(), n, n * n, L.c64(0, 0),
+                       b, None, 0, ws.data_ptr(), wb, s)
+        else:
+            def fn():
+                L.call("euv_zgemm", n, n, n, L.c64(1, 0), None, A.data_ptr(), n, n * n,
+                       B.data_ptr(), n, n * n, L.c64(0, 0), C.data_ptr(), n, n * n, L.c64(0, 0),
+                       b, None, 0, s)
+        ms = _time(fn, a.reps)
+        out.update(ms=ms, complex_tflops=8.0 * n ** 3 * b / (ms / 1e3) / 1e12)
+    else:
+        A += n * torch.eye(n, dtype=torch.complex128, device="cuda")
+        W = torch.empty_like(A)
+        R = torch.randn(b, a.nrhs, n, dtype=torch.complex128, device="cuda", generator=g)
+        X = torch.empty_like(R)
+        piv = torch.empty(b * n, dtype=torch.int32, device="cuda")
+        info = torch.empty(b, dtype=torch.int32, device="cuda")
+
+        def fn():
+            W.copy_(A)
+            X.copy_(R)
+            L.call("euv_lu_factor", n, W.data_ptr(), n, n * n, piv.data_ptr(), info.data_ptr(), b, s)
+            L.call("euv_lu_solve", n, a.nrhs, W.data_ptr(), n, n * n, piv.data_ptr(), X.data_ptr(),
+                   n, n * a.nrhs, b, s)
+        ms = _time(fn, a.reps)
+        out.update(ms=ms, nrhs=a.nrhs)
+    print(json.dumps(out))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
