@@ -305,22 +305,28 @@ __global__ void __launch_bounds__(MX_THREADS, 1)
         tmem_ld16(tmem + lane_addr + (uint32_t)(3 * MX_BN + c0), ci);
         tmem_ld_wait();
         if (row < p.m) {
+          // all 16 reads of C are issued before the first store: a load after
+          // a store through the same pointer type would otherwise wait for it
+          double2 old[16];
+          if (use_beta) {
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+              const int col = n0 + c0 + j;
+              old[j] = col < p.n ? C[row + (long long)col * p.ldc] : make_double2(0.0, 0.0);
+            }
+          }
 #pragma unroll
           for (int j = 0; j < 16; ++j) {
             const int col = n0 + c0 + j;
             if (col < p.n) {
-              double2* cp = C + row + (long long)col * p.ldc;
               // K halves: set 0 at columns [0, 2BN), set 1 (empty if nkb == 1) at [2BN, 4BN)
               const double s1r = nkb > 1 ? (double)__uint_as_float(cr[j]) : 0.0;
               const double s1i = nkb > 1 ? (double)__uint_as_float(ci[j]) : 0.0;
               cplx v = alpha * mk((double)__uint_as_float(vr[j]) + s1r,
                                   (double)__uint_as_float(vi[j]) + s1i);
-              if (use_beta) {
-                double2 o = *cp;
-                v = v + beta * mk(o.x, o.y);
-              }
+              if (use_beta) v = v + beta * mk(old[j].x, old[j].y);
               if (row == col) v = v + dg;
-              *cp = make_double2(v.x, v.y);
+              C[row + (long long)col * p.ldc] = make_double2(v.x, v.y);
             }
           }
         }

@@ -44,23 +44,105 @@ constexpr double kTheta = 1.0;  // ||A||_1 bound for the degree-8 Taylor step
 constexpr int kMaxSteps = 40;
 
 // ---------------------------------------------------------------- mask DFT
-// IND[x + FX*y] = indicator of the pattern pixel (x, y) (header.h:1153-1166).
-__global__ void mask_unpack_kernel(const uint8_t* bits, int ndivx, int ndivy, int fx, int fy,
-                                   int select_vacuum, int y_offset, double2* ind) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  long long total = (long long)fx * fy;
-  if (t >= total) return;
-  int x = (int)(t % fx), y = (int)(t / fx);
-  int meshx = fx / ndivx, meshy = fy / ndivy;
-  int ii = x / meshx;
-  int jj = ndivy - 1 - y / meshy + y_offset;
-  int b = 0;  // rows outside the mask read as absorber
+// The indicator of pattern pixel (x, y), x < FX, y < FY (header.h:1153-1166):
+// the mask bit of column x / meshx and row NDIVY-1 - y / meshy + y_offset
+// (rows outside the mask read as absorber), inverted unless select_vacuum.
+__device__ __forceinline__ double mask_indicator(const uint8_t* bits, int ndivx, int ndivy,
+                                                 int meshx, int meshy, int select_vacuum,
+                                                 int y_offset, int x, int y) {
+  const int ii = x / meshx;
+  const int jj = ndivy - 1 - y / meshy + y_offset;
+  int b = 0;
   if (jj >= 0 && jj < ndivy) {
-    long long bit = (long long)ndivx * jj + ii;
+    const long long bit = (long long)ndivx * jj + ii;
     b = (bits[bit >> 3] >> (7 - (int)(bit & 7))) & 1;
   }
-  double v = select_vacuum ? (double)b : (double)(1 - b);
-  ind[t] = make_double2(v, 0.0);
+  return select_vacuum ? (double)b : (double)(1 - b);
+}
+
+// Stage 1 of the separable DFT, straight from the packed bits:
+//   T[g][m'][x] = sum_y IND_g(x, y) Wy[y + FY m']        (x contiguous)
+// CTA tile: 32 x-columns (lanes) x 64 frequencies (8 warps x 8) for one mask,
+// y streamed through shared memory in chunks of 32.  The indicator is 0/1, so
+// each term is a masked add of a twiddle; one CTA per (x tile, m' tile, mask).
+constexpr int SP_X = 32, SP_M = 64, SP_Y = 32;
+__global__ void __launch_bounds__(256) spectrum_rows_kernel(
+    const uint8_t* bits, long long mask_bytes, int ndivx, int ndivy, int fx, int fy, int mr,
+    int select_vacuum, int y_offset, const double2* Wy, double2* T) {
+  __shared__ double2 ws[SP_Y][SP_M + 1];
+  __shared__ double vs[SP_Y][SP_X];
+  const int g = blockIdx.z;
+  const int x0 = blockIdx.x * SP_X, m0 = blockIdx.y * SP_M;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const uint8_t* mb = bits + (long long)g * mask_bytes;
+  const int meshx = fx / ndivx, meshy = fy / ndivy;
+  double ar[8], ai[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) ar[j] = ai[j] = 0.0;
+  for (int y0 = 0; y0 < fy; y0 += SP_Y) {
+    for (int i = threadIdx.x; i < SP_Y * SP_M; i += 256) {
+      const int yy = i % SP_Y, mm = i / SP_Y, y = y0 + yy, m = m0 + mm;
+      ws[yy][mm] = (y < fy && m < mr) ? Wy[y + (long long)fy * m] : make_double2(0.0, 0.0);
+    }
+    for (int i = threadIdx.x; i < SP_Y * SP_X; i += 256) {
+      const int xx = i % SP_X, yy = i / SP_X, x = x0 + xx, y = y0 + yy;
+      vs[yy][xx] = (x < fx && y < fy)
+                       ? mask_indicator(mb, ndivx, ndivy, meshx, meshy, select_vacuum, y_offset, x, y)
+                       : 0.0;
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int yy = 0; yy < SP_Y; ++yy) {
+      const double a = vs[yy][lane];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const double2 wv = ws[yy][w + 8 * j];
+        ar[j] = fma(a, wv.x, ar[j]);
+        ai[j] = fma(a, wv.y, ai[j]);
+      }
+    }
+    __syncthreads();
+  }
+  const int x = x0 + lane;
+  if (x >= fx) return;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const int m = m0 + w + 8 * j;
+    if (m < mr) T[((long long)g * mr + m) * fx + x] = make_double2(ar[j], ai[j]);
+  }
+}
+
+// Stage 2:  out[g][l' + LR m'] = sum_x Wx[l' + LR x] T[g][m'][x]
+// One CTA per (m', mask); the T row is staged in shared memory, threads own l'.
+constexpr int SC_THREADS = 64, SC_X = 256;
+__global__ void __launch_bounds__(SC_THREADS) spectrum_cols_kernel(int fx, int lr, int mr,
+                                                                   const double2* Wx,
+                                                                   const double2* T,
+                                                                   double2* out) {
+  __shared__ double2 ts[SC_X];
+  const int m = blockIdx.x, g = blockIdx.y;
+  const double2* t = T + ((long long)g * mr + m) * fx;
+  for (int l0 = 0; l0 < lr; l0 += SC_THREADS) {
+    const int l = l0 + threadIdx.x;
+    double sr = 0.0, si = 0.0;
+    for (int x0 = 0; x0 < fx; x0 += SC_X) {
+      __syncthreads();
+      for (int i = threadIdx.x; i < SC_X; i += SC_THREADS)
+        ts[i] = x0 + i < fx ? t[x0 + i] : make_double2(0.0, 0.0);
+      __syncthreads();
+      if (l < lr) {
+        const int xe = fx - x0 < SC_X ? fx - x0 : SC_X;
+        const double2* wx = Wx + l + (long long)lr * x0;
+#pragma unroll 8
+        for (int xx = 0; xx < xe; ++xx) {
+          const double2 a = wx[(long long)lr * xx], b = ts[xx];
+          sr = fma(a.x, b.x, fma(-a.y, b.y, sr));
+          si = fma(a.x, b.y, fma(a.y, b.x, si));
+        }
+      }
+    }
+    if (l < lr) out[(long long)g * lr * mr + l + (long long)lr * m] = make_double2(sr, si);
+  }
 }
 
 // W[r + rows*c] = scale * exp(-2 pi i ((f*g) mod fdiv)/fdiv) with f = r - roff
@@ -847,18 +929,19 @@ extern "C" int euv_amp(const euv_amp_desc* d, const euv_c64* d_spectra, euv_c64*
 // ------------------------------------------------------------------ spectrum
 extern "C" size_t euv_mask_spectrum_workspace_bytes(int n_masks, int ndivx, int ndivy, int fdivx,
                                                     int fdivy, int lh, int mh) {
-  (void)n_masks;
   (void)ndivx;
   (void)ndivy;
   const size_t lr = 2 * (size_t)lh + 1, mr = 2 * (size_t)mh + 1;
   Bump bp{nullptr, (size_t)-1, 0, true};
-  bp.take<double2>((size_t)fdivx * fdivy);
-  bp.take<double2>((size_t)fdivx * mr);
   bp.take<double2>((size_t)fdivy * mr);
   bp.take<double2>(lr * (size_t)fdivx);
+  bp.take<double2>((size_t)(n_masks > 1 ? n_masks : 1) * mr * fdivx);
   return bp.off;
 }
 
+// Masks are transformed in groups that fit the workspace (all of them when it
+// was sized by euv_mask_spectrum_workspace_bytes for n_masks): two launches per
+// group after the two twiddle tables.
 extern "C" int euv_mask_spectrum(const uint8_t* d_bits, int n_masks, int ndivx, int ndivy,
                                  int fdivx, int fdivy, int lh, int mh, int select_vacuum,
                                  int y_offset, euv_c64* d_out, void* d_work, size_t work_bytes, void* stream_) {
@@ -871,14 +954,17 @@ extern "C" int euv_mask_spectrum(const uint8_t* d_bits, int n_masks, int ndivx, 
   cudaStream_t stream = (cudaStream_t)stream_;
   const int lr = 2 * lh + 1, mr = 2 * mh + 1;
   Bump bp{reinterpret_cast<char*>(d_work), work_bytes, 0, true};
-  double2* ind = bp.take<double2>((size_t)fdivx * fdivy);
-  double2* T = bp.take<double2>((size_t)fdivx * mr);
   double2* Wy = bp.take<double2>((size_t)fdivy * mr);
   double2* Wx = bp.take<double2>((size_t)lr * fdivx);
-  if (!d_work || !bp.ok) {
+  const size_t per_mask = ((size_t)mr * fdivx * sizeof(double2) + 255) & ~(size_t)255;
+  const size_t left = bp.ok && work_bytes > bp.off ? work_bytes - bp.off : 0;
+  long long group = (long long)(left / per_mask);
+  if (group > 65535) group = 65535;  // grid z / y limit
+  if (!d_work || !bp.ok || group < 1) {
     euv_set_error("euv_mask_spectrum: workspace too small");
     return EUV_ERR_WORKSPACE;
   }
+  double2* T = reinterpret_cast<double2*>(reinterpret_cast<char*>(d_work) + bp.off);
   // Wy[y + FY m'] = exp(-2 pi i m y / FY) ; Wx[l' + LR x] = exp(-2 pi i l x/FX)/(FX FY)
   twiddle_kernel<<<grid1((long long)fdivy * mr, 256), 256, 0, stream>>>(fdivy, mr, 0, mh, fdivy, 0,
                                                                         1.0, Wy);
@@ -887,18 +973,16 @@ extern "C" int euv_mask_spectrum(const uint8_t* d_bits, int n_masks, int ndivx, 
       lr, fdivx, lh, 0, fdivx, 1, 1.0 / ((double)fdivx * (double)fdivy), Wx);
   EUV_LAUNCH_CHECK();
   const long long mask_bytes = (long long)ndivx * ndivy / 8;
-  const cplx one = mk(1.0, 0.0), zero = mk(0.0, 0.0);
-  for (int b = 0; b < n_masks; ++b) {
-    mask_unpack_kernel<<<grid1((long long)fdivx * fdivy, 256), 256, 0, stream>>>(
-        d_bits + b * mask_bytes, ndivx, ndivy, fdivx, fdivy, select_vacuum, y_offset, ind);
+  for (long long g0 = 0; g0 < n_masks; g0 += group) {
+    const int ng = (int)(n_masks - g0 < group ? n_masks - g0 : group);
+    dim3 g1((fdivx + SP_X - 1) / SP_X, (mr + SP_M - 1) / SP_M, ng);
+    spectrum_rows_kernel<<<g1, 256, 0, stream>>>(d_bits + g0 * mask_bytes, mask_bytes, ndivx,
+                                                  ndivy, fdivx, fdivy, mr, select_vacuum,
+                                                  y_offset, Wy, T);
     EUV_LAUNCH_CHECK();
-    int rc = zgemm(fdivx, mr, fdivy, one, nullptr, ind, fdivx, 0, Wy, fdivy, 0, zero, T, fdivx, 0,
-                   zero, 1, nullptr, 0, stream);
-    if (rc) return rc;
-    rc = zgemm(lr, mr, fdivx, one, nullptr, Wx, lr, 0, T, fdivx, 0, zero,
-               reinterpret_cast<double2*>(d_out) + (long long)b * lr * mr, lr, 0, zero, 1, nullptr,
-               0, stream);
-    if (rc) return rc;
+    spectrum_cols_kernel<<<dim3(mr, ng), SC_THREADS, 0, stream>>>(
+        fdivx, lr, mr, Wx, T, reinterpret_cast<double2*>(d_out) + g0 * lr * mr);
+    EUV_LAUNCH_CHECK();
   }
   return EUV_OK;
 }

@@ -163,24 +163,32 @@ __global__ void __launch_bounds__(GTHREADS, 2) zgemm_kernel(GemmArgs p) {
   const bool use_beta = (p.beta.x != 0.0 || p.beta.y != 0.0);
   const cplx dg = mk(p.diag.x, p.diag.y);
 #pragma unroll
-  for (int mi = 0; mi < 4; ++mi)
+  for (int mi = 0; mi < 4; ++mi) {
+    const int row = m0 + wm + mi * 8 + (lane >> 2);
+    // the 8 reads of C for this row block are issued before its stores (a
+    // load after a store through the same pointer type would wait for it)
+    double2 old[4][2];
 #pragma unroll
     for (int ni = 0; ni < 4; ++ni)
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
-        int row = m0 + wm + mi * 8 + (lane >> 2);
-        int col = n0 + wn + ni * 8 + (lane & 3) * 2 + e;
+        const int col = n0 + wn + ni * 8 + (lane & 3) * 2 + e;
+        old[ni][e] = (use_beta && row < p.m && col < p.n) ? C[row + (long long)col * p.ldc]
+                                                          : make_double2(0.0, 0.0);
+      }
+#pragma unroll
+    for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int col = n0 + wn + ni * 8 + (lane & 3) * 2 + e;
         if (row < p.m && col < p.n) {
-          double2* cp = C + row + (long long)col * p.ldc;
           cplx v = alpha * mk(accr[mi][ni][e], acci[mi][ni][e]);
-          if (use_beta) {
-            double2 o = *cp;
-            v = v + beta * mk(o.x, o.y);
-          }
+          if (use_beta) v = v + beta * mk(old[ni][e].x, old[ni][e].y);
           if (row == col) v = v + dg;
-          *cp = make_double2(v.x, v.y);
+          C[row + (long long)col * p.ldc] = make_double2(v.x, v.y);
         }
       }
+  }
 }
 
 int zgemm_launch(const GemmArgs& p, int batch, cudaStream_t stream) {
