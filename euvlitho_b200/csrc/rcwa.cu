@@ -40,7 +40,15 @@ int gemm_mixed(int m, int n, int k, cplx alpha, const double* scale, const doubl
                const int* steps, int step, void* work, size_t work_bytes, cudaStream_t stream);
 size_t gemm_mixed_workspace_bytes(int m, int n, int k, int batch);
 
-constexpr double kTheta = 1.0;  // ||A||_1 bound for the degree-8 Taylor step
+// ||A||_1 bound for the degree-8 Taylor step of cos/sin(sqrt(A)): the dropped
+// term is ~theta^9/18!, 1.6e-16 at theta = 1 (FP64) and 4e-11 at theta = 4,
+// which the mixed form uses (its TF32x3 products carry ~1e-7 relative error,
+// and each double-angle step saved also saves its error growth).
+constexpr double kThetaFp64 = 1.0;
+constexpr double kThetaMixed = 4.0;
+inline double theta_for(int precision) {
+  return precision == EUV_PREC_MIXED ? kThetaMixed : kThetaFp64;
+}
 constexpr int kMaxSteps = 40;
 
 // ---------------------------------------------------------------- mask DFT
@@ -348,14 +356,14 @@ __global__ void norm1_kernel(int n, const double2* D, double* norm) {
 }
 
 // m = smallest m >= 0 with norm*(d/2^m)^2 <= theta (capped at m_max); h = d/2^m.
-__global__ void scale_kernel(int batch, const double* norm, const double* thick, int m_max,
+__global__ void scale_kernel(int batch, double theta, const double* norm, const double* thick, int m_max,
                              int* steps, double* h, double* h2, double* h4, int* capped) {
   int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= batch) return;
   double d = thick[b];
   double v = norm[b] * d * d;
   int m = 0;
-  while (v > kTheta && m < kMaxSteps) {
+  while (v > theta && m < kMaxSteps) {
     v *= 0.25;
     ++m;
   }
@@ -545,7 +553,8 @@ int matfun(int n, int batch, const double2* D, const double* thick, double2** pc
   dim3 gn(grid1((long long)n * 32, 256), batch);
   norm1_kernel<<<gn, 256, 0, stream>>>(n, D, w.norm);
   EUV_LAUNCH_CHECK();
-  scale_kernel<<<grid1(batch, 128), 128, 0, stream>>>(batch, w.norm, thick, m_max, w.steps, w.h,
+  scale_kernel<<<grid1(batch, 128), 128, 0, stream>>>(batch, theta_for(gemm.precision), w.norm,
+                                                      thick, m_max, w.steps, w.h,
                                                       w.h2, w.h4, w.capped);
   EUV_LAUNCH_CHECK();
   const cplx one = mk(1.0, 0.0), zero = mk(0.0, 0.0);
@@ -586,6 +595,7 @@ int matfun(int n, int batch, const double2* D, const double* thick, double2** pc
 // Upper bound of max_b ||D_b||_1 from the config (Parseval: the window sum of
 // |F| is at most sqrt(window size)); used to bound the double-angle steps.
 static int derive_m_max(const euv_amp_desc* d) {
+  const double theta = theta_for(d->precision);
   const double k = d->k;
   const int lr2 = 4 * d->lmax + 1, mr2 = 4 * d->mmax + 1;
   const double S = sqrt((double)lr2 * (double)mr2);
@@ -608,7 +618,7 @@ static int derive_m_max(const euv_amp_desc* d) {
                     kxm * kxm + kym * kym);
     double v = bound * d->dabs[n] * d->dabs[n];
     int m = 0;
-    while (v > kTheta && m < kMaxSteps) {
+    while (v > theta && m < kMaxSteps) {
       v *= 0.25;
       ++m;
     }
