@@ -8,10 +8,12 @@
 // Blocked right-looking LU, panel width LU_NB:
 //   panel  : one CTA per matrix factors columns [j0, j0+nb) of rows [j0, n)
 //            (pivot = first max of |re|+|im| as LAPACK izamax, row swap inside
-//            the panel, scale, rank-1 update), in global memory (L2 resident);
+//            the panel, scale, rank-1 update), sub-panels in registers;
 //   laswp  : the panel's row swaps applied to the other columns;
 //   trsm   : U12 = L11^-1 A12 (unit lower, L11 staged in shared memory);
 //   update : A22 -= L21 U12 with the batched DMMA zgemm.
+// Solve: the row swaps on B, then one launch that keeps 8 (or fewer, for large
+// n) columns of X in shared memory per CTA through both substitutions.
 #include "common.cuh"
 
 namespace euv {
@@ -397,12 +399,215 @@ int lu_factor(int n, double2* A, long long lda, long long sa, int* ipiv, int* in
   return EUV_OK;
 }
 
+// Forward (unit lower L) and backward (upper U) substitution of RC right-hand
+// sides per CTA with X resident in shared memory (xs[c*n + r]) for the whole
+// solve; L and U are streamed once per CTA in blocks of LS_BLK rows/columns:
+//   diagonal block : staged in shared memory (its loads issued during the
+//                    previous block's update); warp c solves column c, lane i
+//                    = block row i, each solved entry broadcast by shuffle;
+//   off-diagonal   : x(r) -= T(r, block) x(block) for the rows below (forward)
+//                    or above (backward).  RC = 8 runs it on the FP64 tensor
+//                    path: 8-row tiles x 8 right-hand sides x K = 4 DMMAs, four
+//                    per complex step, two tiles' loads in flight per warp.
+// Replaces 2*ceil(n/32) trsm launches + as many K=32 GEMMs per solve.
+constexpr int LS_THREADS = 512;
+constexpr int LS_WARPS = LS_THREADS / 32;
+constexpr int LS_BLK = 32;
+constexpr size_t LS_SMEM_MAX = 200 * 1024;
+
+__device__ __forceinline__ void dmma884(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+// Two elements per thread of the diagonal block at (j0, j0), zero outside jb.
+struct DiagPrefetch {
+  double2 v[2];
+  __device__ __forceinline__ void load(const double2* LU, long long lda, int j0, int jb, int tid) {
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const int i = tid + k * LS_THREADS, r = i % LS_BLK, q = i / LS_BLK;
+      v[k] = (r < jb && q < jb) ? LU[j0 + r + (long long)(j0 + q) * lda] : make_double2(0.0, 0.0);
+    }
+  }
+  __device__ __forceinline__ void store(double2 (*ds)[LS_BLK + 1], int tid) const {
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const int i = tid + k * LS_THREADS;
+      ds[i % LS_BLK][i / LS_BLK] = v[k];
+    }
+  }
+};
+static_assert(2 * LS_THREADS == LS_BLK * LS_BLK, "DiagPrefetch covers the block");
+
+// xs[c*n + r] -= sum_{q<jb} T(r, j0+q) xs[c*n + j0+q], r in [r_lo, r_hi), c < RC
+template <int RC>
+__device__ __forceinline__ void update_rows(double2* xs, int n, const double2* LU, long long lda,
+                                            int j0, int jb, int r_lo, int r_hi, int tid) {
+  if constexpr (RC == 8) {
+    const int lane = tid & 31, warp = tid >> 5, kq = lane & 3, g = lane >> 2;
+    double br[8], bi[8];  // B fragments: x(j0 + 4ks + kq) of right-hand side g
+#pragma unroll
+    for (int ks = 0; ks < 8; ++ks) {
+      const int q = 4 * ks + kq;
+      const double2 v = q < jb ? xs[g * n + j0 + q] : make_double2(0.0, 0.0);
+      br[ks] = v.x;
+      bi[ks] = v.y;
+    }
+    const int ntiles = (r_hi - r_lo + 7) / 8;
+    for (int t = warp; t < ntiles; t += 2 * LS_WARPS) {
+      double2 a[2][8];
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const int tt = t + u * LS_WARPS, r = r_lo + tt * 8 + g;
+        const bool rok = tt < ntiles && r < r_hi;
+#pragma unroll
+        for (int ks = 0; ks < 8; ++ks) {
+          const int q = 4 * ks + kq;
+          a[u][ks] = (rok && q < jb) ? LU[r + (long long)(j0 + q) * lda] : make_double2(0.0, 0.0);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const int tt = t + u * LS_WARPS;
+        if (tt >= ntiles) break;  // warp-uniform
+        double cr0 = 0.0, cr1 = 0.0, ci0 = 0.0, ci1 = 0.0;
+#pragma unroll
+        for (int ks = 0; ks < 8; ++ks) {
+          dmma884(cr0, cr1, a[u][ks].x, br[ks]);
+          dmma884(cr0, cr1, -a[u][ks].y, bi[ks]);
+          dmma884(ci0, ci1, a[u][ks].x, bi[ks]);
+          dmma884(ci0, ci1, a[u][ks].y, br[ks]);
+        }
+        const int r = r_lo + tt * 8 + g;
+        if (r < r_hi) {
+          double2* p0 = &xs[(2 * kq) * n + r];
+          double2* p1 = &xs[(2 * kq + 1) * n + r];
+          const double2 o0 = *p0, o1 = *p1;
+          *p0 = make_double2(o0.x - cr0, o0.y - ci0);
+          *p1 = make_double2(o1.x - cr1, o1.y - ci1);
+        }
+      }
+    }
+  } else {
+    for (int r = r_lo + tid; r < r_hi; r += LS_THREADS) {
+      cplx acc[RC];
+#pragma unroll
+      for (int c = 0; c < RC; ++c) acc[c] = mk(0.0, 0.0);
+#pragma unroll 8
+      for (int q = 0; q < jb; ++q) {
+        const cplx lv = ld2(&LU[r + (long long)(j0 + q) * lda]);
+#pragma unroll
+        for (int c = 0; c < RC; ++c) acc[c] = acc[c] + lv * ld2(&xs[c * n + j0 + q]);
+      }
+#pragma unroll
+      for (int c = 0; c < RC; ++c) st2(&xs[c * n + r], ld2(&xs[c * n + r]) - acc[c]);
+    }
+  }
+}
+
+template <int RC>
+__global__ void __launch_bounds__(LS_THREADS) lu_subst_kernel(int n, int nrhs, const double2* LU,
+                                                              long long lda, long long sa,
+                                                              double2* B, long long ldb,
+                                                              long long sb) {
+  extern __shared__ double2 xs[];
+  __shared__ double2 ds[LS_BLK][LS_BLK + 1];
+  const int b = blockIdx.y, c0 = blockIdx.x * RC;
+  const int nc = (nrhs - c0) < RC ? (nrhs - c0) : RC;
+  LU += (long long)b * sa;
+  B += (long long)b * sb;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  DiagPrefetch pf;
+  pf.load(LU, lda, 0, n < LS_BLK ? n : LS_BLK, tid);
+  for (int i = tid; i < RC * n; i += LS_THREADS) {
+    const int c = i / n, r = i - c * n;
+    xs[i] = c < nc ? B[r + (long long)(c0 + c) * ldb] : make_double2(0.0, 0.0);
+  }
+  pf.store(ds, tid);
+  __syncthreads();
+  // ---- forward: L y = b
+  for (int j0 = 0; j0 < n; j0 += LS_BLK) {
+    const int jb = (n - j0) < LS_BLK ? (n - j0) : LS_BLK;
+    if (warp < nc) {
+      double2* xc = xs + (long long)warp * n + j0;
+      cplx x = lane < jb ? ld2(&xc[lane]) : mk(0.0, 0.0);
+#pragma unroll
+      for (int q = 0; q < LS_BLK; ++q) {
+        const cplx xq = mk(__shfl_sync(0xffffffffu, x.x, q), __shfl_sync(0xffffffffu, x.y, q));
+        if (lane > q && lane < jb) x = x - ld2(&ds[lane][q]) * xq;
+      }
+      if (lane < jb) st2(&xc[lane], x);
+    }
+    __syncthreads();
+    // next diagonal block: the forward pass's successor, or the backward pass's first
+    const int jn = j0 + LS_BLK < n ? j0 + LS_BLK : ((n - 1) / LS_BLK) * LS_BLK;
+    pf.load(LU, lda, jn, (n - jn) < LS_BLK ? (n - jn) : LS_BLK, tid);
+    update_rows<RC>(xs, n, LU, lda, j0, jb, j0 + jb, n, tid);
+    pf.store(ds, tid);
+    __syncthreads();
+  }
+  // ---- backward: U x = y
+  for (int j0 = ((n - 1) / LS_BLK) * LS_BLK; j0 >= 0; j0 -= LS_BLK) {
+    const int jb = (n - j0) < LS_BLK ? (n - j0) : LS_BLK;
+    if (warp < nc) {
+      double2* xc = xs + (long long)warp * n + j0;
+      cplx x = lane < jb ? ld2(&xc[lane]) : mk(0.0, 0.0);
+      // each lane's reciprocal pivot, off the serial chain below
+      const cplx rinv = lane < jb ? cdiv(mk(1.0, 0.0), ld2(&ds[lane][lane])) : mk(0.0, 0.0);
+#pragma unroll
+      for (int q = LS_BLK - 1; q >= 0; --q) {
+        if (q < jb) {  // warp-uniform
+          if (lane == q) x = x * rinv;
+          const cplx xq = mk(__shfl_sync(0xffffffffu, x.x, q), __shfl_sync(0xffffffffu, x.y, q));
+          if (lane < q) x = x - ld2(&ds[lane][q]) * xq;
+        }
+      }
+      if (lane < jb) st2(&xc[lane], x);
+    }
+    __syncthreads();
+    if (j0 > 0) pf.load(LU, lda, j0 - LS_BLK, LS_BLK, tid);
+    update_rows<RC>(xs, n, LU, lda, j0, jb, 0, j0, tid);
+    if (j0 > 0) pf.store(ds, tid);
+    __syncthreads();
+  }
+  for (int i = tid; i < RC * n; i += LS_THREADS) {
+    const int c = i / n, r = i - c * n;
+    if (c < nc) B[r + (long long)(c0 + c) * ldb] = xs[i];
+  }
+}
+
+template <int RC>
+static int launch_subst(int n, int nrhs, const double2* LU, long long lda, long long sa,
+                        double2* B, long long ldb, long long sb, int batch, cudaStream_t stream) {
+  static int smem_done[64];
+  const int smem = (int)((size_t)RC * n * sizeof(double2));
+  EUV_CUDA_TRY(ensure_smem(lu_subst_kernel<RC>, smem, smem_done));
+  dim3 grid((nrhs + RC - 1) / RC, batch);
+  lu_subst_kernel<RC><<<grid, LS_THREADS, smem, stream>>>(n, nrhs, LU, lda, sa, B, ldb, sb);
+  EUV_LAUNCH_CHECK();
+  return EUV_OK;
+}
+
 int lu_solve(int n, int nrhs, const double2* LU, long long lda, long long sa, const int* ipiv,
              double2* B, long long ldb, long long sb, int batch, cudaStream_t stream) {
   if (n <= 0 || nrhs <= 0 || batch <= 0) return EUV_OK;
   dim3 gs((nrhs + 127) / 128, batch);
   lu_laswp_kernel<<<gs, 128, 0, stream>>>(n, nrhs, 0, n, 0, 0, B, ldb, sb, ipiv, n);
   EUV_LAUNCH_CHECK();
+  if (batch <= 65535) {
+    const size_t col = (size_t)n * sizeof(double2);
+    if (8 * col <= LS_SMEM_MAX && nrhs >= 8)
+      return launch_subst<8>(n, nrhs, LU, lda, sa, B, ldb, sb, batch, stream);
+    if (4 * col <= LS_SMEM_MAX && nrhs >= 4)
+      return launch_subst<4>(n, nrhs, LU, lda, sa, B, ldb, sb, batch, stream);
+    if (2 * col <= LS_SMEM_MAX && nrhs >= 2)
+      return launch_subst<2>(n, nrhs, LU, lda, sa, B, ldb, sb, batch, stream);
+    if (col <= LS_SMEM_MAX)
+      return launch_subst<1>(n, nrhs, LU, lda, sa, B, ldb, sb, batch, stream);
+  }
+  // n too large for one column of X in shared memory: blocked trsm + GEMM
   // forward: L y = b (unit lower)
   for (int j0 = 0; j0 < n; j0 += LU_NB) {
     const int jb = (n - j0) < LU_NB ? (n - j0) : LU_NB;

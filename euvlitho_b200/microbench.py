@@ -84,11 +84,13 @@ def _time(fn, reps: int) -> float:
         fn()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.profiler.start()
     e0.record()
     for _ in range(reps):
         fn()
     e1.record()
     torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
     return e0.elapsed_time(e1) / reps
 
 
