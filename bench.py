@@ -42,6 +42,8 @@ def _args():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-library-path", action="store_true",
+                    help="skip timing the reference's cuSOLVER/cuBLAS/cuFFT sequence")
     return ap.parse_args()
 
 
@@ -164,8 +166,8 @@ def dominant_kernel_roofline(plan, U, precision, dev, stream, L):
     mixed: the tcgen05 TF32x3 complex GEMM; algorithmic work = 24*N^3 TF32
     FLOP per unit (3 split products x 4 real products x 2N^3), peak = cuBLAS
     TF32 GEMM measured in this run.  fp64: the DMMA complex GEMM, 8*N^3 FLOP
-    per unit, peak = cuBLAS ZGEMM measured in this run.  (MEASURED_PEAKS.json
-    holds BF16 and HBM peaks only.)"""
+    per unit, peak = cuBLAS ZGEMM measured in this run (the pool's measured
+    peaks cover BF16 and HBM only)."""
     import torch
     N = plan.orders.n
     A = torch.randn(U, N, N, dtype=torch.complex128, device=dev)
@@ -211,6 +213,83 @@ def dominant_kernel_roofline(plan, U, precision, dev, stream, L):
     out.update({"achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                 "ms_per_launch": ms, "algorithmic_flop_per_launch": flop})
     return out
+
+
+def library_path_sample(plan, masks_dev, dev, units_per_clip: int, n_src_images: int):
+    """The reference's own GPU library path, timed on this device for one Bloch
+    unit (family, polarisation) of the bench workload and one clip's Abbe FFTs.
+
+    Per unit the reference calls, on N x N complex matrices (N = 961 here):
+    one eigendecomposition with right vectors (cusolverDnXgeev, header.h:837-882),
+    three inverses (matinv: br1, B1 and U0, header.h:933-976, 1053-1055, 1407)
+    and five products (Sigma br1 and the tail, header.h:1002-1017, 1355-1465).
+    The same sequence runs here through torch.linalg (eig, inv) and torch.matmul
+    (cuBLAS ZGEMM); the eigendecomposition takes the workload's own D = k^2 eps
+    - i eta kx+ - kxy^2 (header.h:806-833), built from this library's mask
+    spectrum.  Abbe: 3 inverse 2-D FFTs of the XDIV x XDIV grid per source image
+    (cuFFT Z2Z, intensity.cpp:359-376), batched into one call here (the
+    reference issues one per source with host copies in between).  Wall clock
+    with a device synchronise on both sides: the eigensolver synchronises
+    with the host.  Returns clips/s = 1 / (units_per_clip x t_unit + t_abbe)."""
+    import cmath
+    import math
+    import torch
+    cfg = plan.cfg
+    li = torch.as_tensor(plan.orders.lidx, device=dev, dtype=torch.long)
+    mi = torch.as_tensor(plan.orders.midx, device=dev, dtype=torch.long)
+    lh, mh = 2 * plan.orders.lmax, 2 * plan.orders.mmax
+    ind = plan.spectra(masks_dev[:1], lh, mh)[0, 0].view(2 * mh + 1, 2 * lh + 1).T
+    eabs = complex(cfg.eabs[0])
+    eps = (eabs - 1.0) * ind
+    eps[lh, mh] += 1.0
+    sig = (1.0 / eabs - 1.0) * ind
+    sig[lh, mh] += 1.0
+    lgrid = torch.arange(-lh, lh + 1, device=dev, dtype=torch.float64).view(-1, 1)
+    eta = (1j * 2 * math.pi / cfg.dx) * lgrid * (cmath.log(eabs) * ind)
+    LL = li[:, None] - li[None, :] + lh
+    MM = mi[:, None] - mi[None, :] + mh
+    kxp = (cfg.kx0 + 2 * math.pi * li / cfg.dx).to(torch.complex128)
+    kyp = (cfg.ky0 + 2 * math.pi * mi / cfg.dy).to(torch.complex128)
+    k = cfg.k
+    D = k * k * eps[LL, MM] - 1j * eta[LL, MM] * kxp[None, :]
+    D.diagonal().sub_(kxp * kxp + kyp * kyp)
+    Sig = sig[LL, MM] * kxp[None, :]
+
+    def unit():
+        _, br1 = torch.linalg.eig(D)
+        cjp = torch.linalg.inv(br1)
+        b1 = 1j * (k * br1 - (kxp[:, None] / k) * (Sig @ br1))
+        cj = torch.linalg.inv(b1)
+        x = cj @ cjp
+        y = cjp @ cj
+        u0i = torch.linalg.inv(x + y)
+        return (x @ u0i) @ y
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            fn()
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t0) / reps
+
+    t_unit = timed(unit, 2)
+    t_eig = timed(lambda: torch.linalg.eig(D), 2)
+    grid = torch.zeros((n_src_images * 3, cfg.xdiv, cfg.xdiv), dtype=torch.complex128, device=dev)
+    t_abbe = timed(lambda: torch.fft.ifft2(grid, norm="forward"), 3)
+    per_clip = units_per_clip * t_unit + t_abbe
+    try:
+        backend = str(torch.backends.cuda.preferred_linalg_library())
+    except Exception:  # reporting only
+        backend = "default"
+    return {"value": 1.0 / per_clip, "unit": "clips/s", "ms_per_unit": t_unit * 1e3,
+            "eig_ms": t_eig * 1e3, "abbe_ms_per_clip": t_abbe * 1e3,
+            "units_per_clip": units_per_clip, "linalg_backend": backend,
+            "calls_per_unit": "eig + 3 inv + 5 ZGEMM of %d x %d (torch.linalg / cuBLAS)"
+                              % (plan.orders.n, plan.orders.n),
+            "abbe": "%d x 3 inverse FFTs of %d^2 (cuFFT, one batched call)"
+                    % (n_src_images, cfg.xdiv)}
 
 
 # ---------------------------------------------------------------- clocks
@@ -363,6 +442,13 @@ def main() -> int:
 
     roofline = dominant_kernel_roofline(plan, b.U, a.precision, dev, stream, L)
 
+    libpath = None
+    if world == 1 and not a.no_library_path:
+        try:
+            libpath = library_path_sample(plan, b.masks, dev, b.U // CLIPS, plan.sdivsum * 2)
+        except Exception as e:  # the baseline is reported, never required
+            libpath = {"error": repr(e)}
+
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         try:
@@ -386,6 +472,7 @@ def main() -> int:
         "speedup_vs_plain": value / plain_value,
         "intensity_err_vs_fp64": intensity_err,
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+        "library_path_fp64": libpath,
         "gpu_launches": int(launches_per_step * a.steps),
         "clocks": clk,
     }
