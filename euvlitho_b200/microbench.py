@@ -8,10 +8,12 @@
 
 Times each library entry point with CUDA events on the launching stream after
 warm-up and prints one JSON line (the commands the ncu summaries in profiles/
-are taken from).  `step` runs one pipeline step of the batched workload
-(1024 nm box, 15 Bloch units per clip and polarisation pair) untimed, then
-`--reps` steps between cudaProfilerStart/Stop, so that
-`ncu --profile-from-start off` lists exactly those steps' launches.
+are taken from).  `step` runs one pipeline step of a preset's workload (the
+batched one by default: 1024 nm clips, N = 961, 3 Bloch families x 2
+polarisations = 6 units per clip) untimed, then `--reps` steps between
+cudaProfilerStart/Stop, so that `ncu --profile-from-start off` lists exactly
+those steps' launches; `--compare` adds the FP64 form's image and the mixed
+form's intensity error against it.
 `summarize` folds an ncu `--csv` launch list of gpu__time_duration.sum into
 launches, total time and share per kernel.
 """
@@ -74,9 +76,24 @@ def _step(a) -> dict:
     e1.record()
     torch.cuda.synchronize()
     torch.cuda.profiler.stop()
-    return {"preset": a.preset, "precision": a.precision, "clips": a.clips, "units": b.U,
-            "ms_per_step": e0.elapsed_time(e1) / a.reps,
-            "launches_per_step": (L.lib().euv_kernel_launches() - n0) // a.reps}
+    out = {"preset": a.preset, "precision": a.precision, "clips": a.clips, "units": b.U,
+           "orders": plan.orders.n, "slices": cfg.nabs,
+           "ms_per_step": e0.elapsed_time(e1) / a.reps,
+           "launches_per_step": (L.lib().euv_kernel_launches() - n0) // a.reps}
+    if a.compare and a.precision != "fp64":
+        img = b.image.clone()
+        del b
+        p64 = Plan(cfg, device=torch.device("cuda"), pols=("X", "Y"), precision="fp64")
+        b64 = p64.intensity_batch(a.clips)
+        b64.masks.copy_(torch.from_numpy(MK.batch(cfg.ndivx, cfg.ndivy, range(a.clips))))
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record()
+        b64.run()
+        t1.record()
+        torch.cuda.synchronize()
+        out["fp64_ms_per_step"] = t0.elapsed_time(t1)
+        out["intensity_err_vs_fp64"] = float((img - b64.image).abs().max() / b64.image.abs().max())
+    return out
 
 
 def _time(fn, reps: int) -> float:
@@ -105,6 +122,8 @@ def main(argv=None) -> int:
     ap.add_argument("--preset", default="batched")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--clips", type=int, default=4)
+    ap.add_argument("--compare", action="store_true",
+                    help="step: also run the FP64 form and report the intensity error")
     a = ap.parse_args(argv)
     if a.kernel == "summarize":
         print(summarize(a.csv))
