@@ -181,7 +181,7 @@ def dominant_kernel_roofline(plan, U, precision, dev, stream, L):
         def gemm():
             L.call("euv_zgemm_tf32x3", N, N, N, L.c64(1, 0), None, A.data_ptr(), N, N * N,
                    B.data_ptr(), N, N * N, L.c64(0, 0), C.data_ptr(), N, N * N, L.c64(0, 0), U,
-                   None, 0, ws.data_ptr(), wb, s)
+                   None, 0, ws.data_ptr(), wb, None, s)
         flop = 24.0 * N ** 3 * U
         ms = _time_ms(gemm, stream, 5)
         X = torch.randn(8192, 8192, dtype=torch.float32, device=dev)

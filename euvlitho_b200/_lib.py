@@ -17,6 +17,11 @@ EUV_ERR_BAD_ARG = 1
 EUV_ERR_CUDA = 2
 EUV_ERR_WORKSPACE = 3
 EUV_ERR_SINGULAR = 4
+EUV_ERR_TIMEOUT = 5
+# bits of a device status word (euv_amp_desc.d_status and friends)
+EUV_STATUS_TIMEOUT = 1
+EUV_STATUS_STEPS_CLAMPED = 2
+EUV_STATUS_SINGULAR = 4
 EUV_MAX_SLICES = 32
 EUV_PREC_FP64 = 0
 EUV_PREC_MIXED = 1
@@ -30,6 +35,7 @@ EXPORTS = (
     "euv_abbe", "euv_m3d_fit",
     "euv_zgemm", "euv_zgemm_tf32x3_workspace_bytes", "euv_zgemm_tf32x3", "euv_lu_workspace_bytes", "euv_lu_factor", "euv_lu_solve",
     "euv_matfun_workspace_bytes", "euv_matfun_cs", "euv_matfun_cs_noalloc",
+    "euv_wait_probe",
 )
 
 
@@ -76,6 +82,7 @@ class AmpDesc(C.Structure):
         ("d_kx0", P), ("d_ky0", P), ("d_polar", P), ("d_spec", P),
         ("n_src", C.c_int), ("d_src_order", P), ("d_src_2kz", P),
         ("precision", C.c_int), ("m_max", C.c_int), ("k0_max", C.c_double),
+        ("d_status", P),
     ]
 
 
@@ -127,7 +134,8 @@ def _declare(lib: C.CDLL) -> None:
     lib.euv_zgemm_tf32x3_workspace_bytes.restype = sz
     lib.euv_zgemm_tf32x3_workspace_bytes.argtypes = [i, i, i, i]
     lib.euv_zgemm_tf32x3.restype = i
-    lib.euv_zgemm_tf32x3.argtypes = [i, i, i, c64, P, P, i, ll, P, i, ll, c64, P, i, ll, c64, i, P, i, P, sz, P]
+    lib.euv_zgemm_tf32x3.argtypes = [i, i, i, c64, P, P, i, ll, P, i, ll, c64, P, i, ll, c64, i, P, i, P, sz,
+                                     P, P]
     lib.euv_lu_workspace_bytes.restype = sz
     lib.euv_lu_workspace_bytes.argtypes = [i, i]
     lib.euv_lu_factor.restype = i
@@ -140,6 +148,8 @@ def _declare(lib: C.CDLL) -> None:
     lib.euv_matfun_cs.argtypes = [i, P, P, P, P, i, i, i, P, sz, P]
     lib.euv_matfun_cs_noalloc.restype = i
     lib.euv_matfun_cs_noalloc.argtypes = [i, P, P, P, P, i, i, P]
+    lib.euv_wait_probe.restype = i
+    lib.euv_wait_probe.argtypes = [P, ll, P, P]
 
 
 def lib() -> C.CDLL:
@@ -163,3 +173,30 @@ def check(fn: str, rc: int) -> None:
 
 def call(fn: str, *args) -> None:
     check(fn, getattr(lib(), fn)(*args))
+
+
+_STATUS_TEXT = (
+    (EUV_STATUS_TIMEOUT, "a bounded device wait gave up (results incomplete)"),
+    (EUV_STATUS_STEPS_CLAMPED, "a unit needed more double-angle steps than m_max"),
+    (EUV_STATUS_SINGULAR, "an LU met an exactly zero pivot"),
+)
+
+
+def status_message(bits: int) -> Optional[str]:
+    """Text for the EUV_STATUS_* bits of a device status word (None if clear)."""
+    if not bits:
+        return None
+    parts = [t for b, t in _STATUS_TEXT if bits & b]
+    rest = bits & ~sum(b for b, _ in _STATUS_TEXT)
+    if rest:
+        parts.append("unknown bits 0x%x" % rest)
+    return "; ".join(parts)
+
+
+def check_status(where: str, bits: int) -> None:
+    """Raise EuvError if a device status word has any bit set."""
+    msg = status_message(int(bits))
+    if msg is not None:
+        code = EUV_ERR_TIMEOUT if bits & EUV_STATUS_TIMEOUT else (
+            EUV_ERR_SINGULAR if bits & EUV_STATUS_SINGULAR else EUV_ERR_CUDA)
+        raise EuvError(where, code, "device status 0x%x: %s" % (int(bits), msg))

@@ -63,6 +63,27 @@ __device__ __forceinline__ void st(euv_c64* p, cplx v) {
 }
 __host__ __device__ __forceinline__ cplx fromc(euv_c64 a) { return mk(a.re, a.im); }
 
+__device__ __forceinline__ unsigned long long globaltimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// The one spin loop of every device wait in the library: polls ready() and,
+// every 256 polls, abort() and the %globaltimer clock.  Returns 1 when ready,
+// 0 when aborted (another role gave up), -1 after limit_ns nanoseconds.
+template <class Ready, class Abort>
+__device__ __forceinline__ int bounded_spin(Ready ready, Abort abort, unsigned long long limit_ns) {
+  const unsigned long long t0 = globaltimer();
+  for (uint32_t it = 0;; ++it) {
+    if (ready()) return 1;
+    if ((it & 255u) == 255u) {
+      if (abort()) return 0;
+      if (globaltimer() - t0 > limit_ns) return -1;
+    }
+  }
+}
+
 }  // namespace euv
 
 #define EUV_CUDA_TRY(expr)                                     \

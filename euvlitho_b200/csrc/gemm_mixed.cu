@@ -23,8 +23,8 @@
 //                a 128x128 tile) and the single-thread MMA issue loop;
 //   warps 2..5 : epilogue, tcgen05.ld of their 32 TMEM lanes (= rows), complex
 //                FP64 result written column by column (coalesced).
-// All waits are bounded (about 2 s); a timeout sets the error word, drains the
-// copies and MMAs in flight, frees TMEM and returns.
+// All waits are bounded (about 2 s); a timeout ORs EUV_STATUS_TIMEOUT into the
+// status word, drains the copies and MMAs in flight, frees TMEM and returns.
 #include <cuda.h>
 #include "common.cuh"
 
@@ -41,8 +41,8 @@ constexpr int MX_BK = 16;  // fp32 elements: 64-byte rows, one 64B swizzle span
 constexpr int MX_STAGES = 3;
 constexpr int MX_PLANES = 4;
 constexpr int MX_A_TILE = MX_BM * MX_BK * 4;  // 8 KB
-constexpr int MX_B_TILE = MX_BN * MX_BK * 4;  // 16 KB
-constexpr int MX_STAGE_BYTES = MX_PLANES * (MX_A_TILE + MX_B_TILE);  // 96 KB
+constexpr int MX_B_TILE = MX_BN * MX_BK * 4;  // 8 KB
+constexpr int MX_STAGE_BYTES = MX_PLANES * (MX_A_TILE + MX_B_TILE);  // 64 KB
 constexpr int MX_THREADS = 192;
 constexpr int MX_TMEM_COLS = 512;
 constexpr size_t MX_SMEM = (size_t)MX_STAGES * MX_STAGE_BYTES + 1024 + 256;
@@ -64,11 +64,6 @@ struct MixedArgs {
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
 }
-__device__ __forceinline__ unsigned long long globaltimer() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
 }
@@ -88,21 +83,18 @@ __device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Bounded wait: false after the deadline (or when another role already gave up).
+// Bounded wait: false after the deadline (the status word gets
+// EUV_STATUS_TIMEOUT) or when another role already gave up.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
                                           int* err) {
-  const unsigned long long t0 = globaltimer();
-  for (uint32_t it = 0;; ++it) {
-    if (mbar_try(bar, parity)) return true;
-    if ((it & 255u) == 255u) {
-      if (*abort_flag) return false;
-      if (globaltimer() - t0 > MX_TIMEOUT_NS) {
-        *abort_flag = 1;
-        atomicExch(err, 1);
-        return false;
-      }
-    }
+  const int r = bounded_spin([&] { return mbar_try(bar, parity); },
+                             [&] { return *abort_flag != 0; }, MX_TIMEOUT_NS);
+  if (r == 1) return true;
+  if (r < 0) {
+    *abort_flag = 1;
+    atomicOr(err, EUV_STATUS_TIMEOUT);
   }
+  return false;
 }
 __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z,
                                             uint64_t* bar) {
@@ -465,7 +457,8 @@ size_t gemm_mixed_workspace_bytes(int m, int n, int k, int batch) {
 int gemm_mixed(int m, int n, int k, cplx alpha, const double* scale, const double2* a,
                long long lda, long long sa, const double2* b, long long ldb, long long sb,
                cplx beta, double2* c, long long ldc, long long sc, cplx diag, int batch,
-               const int* steps, int step, void* work, size_t work_bytes, cudaStream_t stream) {
+               const int* steps, int step, void* work, size_t work_bytes, int* status,
+               cudaStream_t stream) {
   if (m <= 0 || n <= 0 || batch <= 0) return EUV_OK;
   if (k <= 0 || batch > 65535 || (size_t)batch * MX_PLANES > 0x7fffffff) {
     euv_set_error("gemm_mixed: unsupported shape");
@@ -483,8 +476,12 @@ int gemm_mixed(int m, int n, int k, cplx alpha, const double* scale, const doubl
   size_t abytes = ((size_t)batch * MX_PLANES * (size_t)m * kp * 4 + 1023) & ~(size_t)1023;
   float* pb = reinterpret_cast<float*>(w + abytes);
   size_t bbytes = ((size_t)batch * MX_PLANES * (size_t)n * kp * 4 + 1023) & ~(size_t)1023;
-  int* err = reinterpret_cast<int*>(w + abytes + bbytes);
-  EUV_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int), stream));
+  // the caller's sticky status word, else a per-call word in the workspace
+  int* err = status;
+  if (err == nullptr) {
+    err = reinterpret_cast<int*>(w + abytes + bbytes);
+    EUV_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int), stream));
+  }
   {
     dim3 g((m + 31) / 32, (kp + 31) / 32, batch), t(32, 8);
     split_a_kernel<<<g, t, 0, stream>>>(m, k, kp, a, lda, sa, pa, steps, step);
@@ -537,7 +534,7 @@ extern "C" int euv_zgemm_tf32x3(int m, int n, int k, euv_c64 alpha, const double
                                 const euv_c64* d_b, int ldb, long long stride_b, euv_c64 beta,
                                 euv_c64* d_c, int ldc, long long stride_c, euv_c64 diag,
                                 int batch, const int* d_steps, int step, void* d_work,
-                                size_t work_bytes, void* stream) {
+                                size_t work_bytes, int* d_status, void* stream) {
   if (m <= 0 || n <= 0 || k <= 0 || batch <= 0 || lda < m || ldc < m || ldb < k || !d_a ||
       !d_b || !d_c || (d_steps != nullptr && (m != n || m != k))) {
     euv_set_error("euv_zgemm_tf32x3: bad arguments (m=%d n=%d k=%d)", m, n, k);
@@ -546,5 +543,5 @@ extern "C" int euv_zgemm_tf32x3(int m, int n, int k, euv_c64 alpha, const double
   return gemm_mixed(m, n, k, fromc(alpha), d_scale, reinterpret_cast<const double2*>(d_a), lda,
                     stride_a, reinterpret_cast<const double2*>(d_b), ldb, stride_b, fromc(beta),
                     reinterpret_cast<double2*>(d_c), ldc, stride_c, fromc(diag), batch, d_steps,
-                    step, d_work, work_bytes, (cudaStream_t)stream);
+                    step, d_work, work_bytes, d_status, (cudaStream_t)stream);
 }

@@ -37,7 +37,8 @@ int lu_solve(int n, int nrhs, const double2* LU, long long lda, long long sa, co
 int gemm_mixed(int m, int n, int k, cplx alpha, const double* scale, const double2* a,
                long long lda, long long sa, const double2* b, long long ldb, long long sb,
                cplx beta, double2* c, long long ldc, long long sc, cplx diag, int batch,
-               const int* steps, int step, void* work, size_t work_bytes, cudaStream_t stream);
+               const int* steps, int step, void* work, size_t work_bytes, int* status,
+               cudaStream_t stream);
 size_t gemm_mixed_workspace_bytes(int m, int n, int k, int batch);
 
 // ||A||_1 bound for the degree-8 Taylor step of cos/sin(sqrt(A)): the dropped
@@ -369,7 +370,7 @@ __global__ void scale_kernel(int batch, double theta, const double* norm, const 
   }
   if (m > m_max) {
     m = m_max;
-    if (capped) atomicExch(capped, 1);
+    if (capped) atomicOr(capped, EUV_STATUS_STEPS_CLAMPED);
   }
   double hh = ldexp(d, -m);
   steps[b] = m;
@@ -515,20 +516,27 @@ __global__ void fill_f64_kernel(double* p, int n, double v) {
   if (i < n) p[i] = v;
 }
 
-// GEMM dispatch by precision (FP64 DMMA, or BF16x3 tensor cores for the bulk
-// products of the mixed form).
+// An LU's zero pivots (info != 0) as EUV_STATUS_SINGULAR in the status word.
+__global__ void flag_singular_kernel(const int* info, int n, int* status) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && info[i] != 0) atomicOr(status, EUV_STATUS_SINGULAR);
+}
+
+// GEMM dispatch by precision (FP64 DMMA, or TF32x3 tcgen05 tensor cores for
+// the bulk products of the mixed form; `status` receives EUV_STATUS_TIMEOUT).
 struct Gemm {
   int precision;
   void* mwork;
   size_t mbytes;
   cudaStream_t stream;
+  int* status = nullptr;
   int operator()(int m, int n, int k, cplx alpha, const double* scale, const double2* a,
                  long long lda, long long sa, const double2* b, long long ldb, long long sb,
                  cplx beta, double2* c, long long ldc, long long sc, cplx diag, int batch,
                  const int* steps = nullptr, int step = 0) const {
     if (precision == EUV_PREC_MIXED)
       return gemm_mixed(m, n, k, alpha, scale, a, lda, sa, b, ldb, sb, beta, c, ldc, sc, diag,
-                        batch, steps, step, mwork, mbytes, stream);
+                        batch, steps, step, mwork, mbytes, status, stream);
     return zgemm(m, n, k, alpha, scale, a, lda, sa, b, ldb, sb, beta, c, ldc, sc, diag, batch,
                  steps, step, stream);
   }
@@ -752,10 +760,13 @@ extern "C" int euv_amp(const euv_amp_desc* d, const euv_c64* d_spectra, euv_c64*
   const cplx one = mk(1.0, 0.0), zero = mk(0.0, 0.0), mi = mk(0.0, -1.0);
   int m_max = d->m_max > 0 ? d->m_max : derive_m_max(d);
   if (m_max > kMaxSteps) m_max = kMaxSteps;
-  Gemm gemm{d->precision, w.mwork, w.mbytes, stream};
+  // device-detected conditions go to the caller's status word, else to a
+  // workspace word nobody reads
+  int* status = d->d_status ? d->d_status : w.capped;
+  Gemm gemm{d->precision, w.mwork, w.mbytes, stream, status};
   int rc;
 
-  EUV_CUDA_TRY(cudaMemsetAsync(w.capped, 0, sizeof(int), stream));
+  if (!d->d_status) EUV_CUDA_TRY(cudaMemsetAsync(w.capped, 0, sizeof(int), stream));
   // per-slice thickness arrays [slice][unit]
   for (int n = 0; n < NS; ++n) {
     fill_f64_kernel<<<grid1(U, 256), 256, 0, stream>>>(w.thick + (size_t)n * U, U, d->dabs[n]);
@@ -805,7 +816,7 @@ extern "C" int euv_amp(const euv_amp_desc* d, const euv_c64* d_spectra, euv_c64*
   EUV_LAUNCH_CHECK();
 
   const double2* spec = reinterpret_cast<const double2*>(d_spectra);
-  MatfunBufs mb{w.P2, w.P3, w.P4, w.T1, w.W, w.norm, w.h, w.h2, w.h4, w.steps, w.capped};
+  MatfunBufs mb{w.P2, w.P3, w.P4, w.T1, w.W, w.norm, w.h, w.h2, w.h4, w.steps, status};
   // Mixed form: G^-1 by the Euler product (I - E)^-1 = prod_f (I + E^(2^f)),
   // f < euler_f, when the config bound on ||E||_2 makes it converge fast.
   const int euler_f = d->precision == EUV_PREC_MIXED ? euler_factors(d) : 0;
@@ -857,6 +868,8 @@ extern "C" int euv_amp(const euv_amp_desc* d, const euv_c64* d_spectra, euv_c64*
       diag_kernel<<<ge, bs, 0, stream>>>(N, w.gx2, w.Z);
       EUV_LAUNCH_CHECK();
       if ((rc = lu_factor(N, w.G, N, nn, w.ipiv, w.info, U, stream))) return rc;
+      flag_singular_kernel<<<grid1(U, 256), 256, 0, stream>>>(w.info, U, status);
+      EUV_LAUNCH_CHECK();
       if ((rc = lu_solve(N, N, w.G, N, nn, w.ipiv, w.Z, N, nn, U, stream))) return rc;
       Zp = w.Z;
     } else if (d->refresh_sigma && euler_f > 0) {
@@ -880,6 +893,8 @@ extern "C" int euv_amp(const euv_amp_desc* d, const euv_c64* d_spectra, euv_c64*
       EUV_LAUNCH_CHECK();
       if ((rc = gemm(N, N, N, one, nullptr, w.Gp, N, nn, X, N, nn, zero, w.Z, N, nn, zero, U))) return rc;
       if ((rc = lu_factor(N, w.G, N, nn, w.ipiv, w.info, U, stream))) return rc;
+      flag_singular_kernel<<<grid1(U, 256), 256, 0, stream>>>(w.info, U, status);
+      EUV_LAUNCH_CHECK();
       if ((rc = lu_solve(N, N, w.G, N, nn, w.ipiv, w.Z, N, nn, U, stream))) return rc;
       Zp = w.Z;
     }
@@ -920,6 +935,8 @@ extern "C" int euv_amp(const euv_amp_desc* d, const euv_c64* d_spectra, euv_c64*
   u0_kernel<<<ge, bs, 0, stream>>>(N, w.klm, X, Y, w.G);
   EUV_LAUNCH_CHECK();
   if ((rc = lu_factor(N, w.G, N, nn, w.ipiv, w.info, U, stream))) return rc;
+  flag_singular_kernel<<<grid1(U, 256), 256, 0, stream>>>(w.info, U, status);
+  EUV_LAUNCH_CHECK();
   const int ns = d->n_src;
   if (ns > 0) {
     dim3 gs(grid1((long long)N * ns, bs), U);

@@ -113,6 +113,8 @@ class Plan:
         self._abbe_tables = None
         self._m3d_tables = None
         self._batches: Dict[Tuple[int, int], "IntensityBatch"] = {}
+        # device status word of the plan's own ampS calls (EUV_STATUS_* bits)
+        self.status = torch.zeros(1, dtype=torch.int32, device=dev)
 
     # ------------------------------------------------------------ helpers
     def _i32(self, a) -> torch.Tensor:
@@ -167,7 +169,7 @@ class Plan:
 
     # ------------------------------------------------------------ ampS
     def amp_desc(self, orders: OrderSet, t_l, t_m, kx0, ky0, polar, spec_of_unit,
-                 src_order, src_2kz, keep) -> L.AmpDesc:
+                 src_order, src_2kz, keep, status: Optional[torch.Tensor] = None) -> L.AmpDesc:
         cfg = self.cfg
         d = L.AmpDesc()
         d.n_orders = orders.n
@@ -187,8 +189,15 @@ class Plan:
         d.precision = self.precision
         d.m_max = 0
         d.k0_max = float(max(kx0.abs().max().item(), ky0.abs().max().item()))
+        d.d_status = _ptr(self.status if status is None else status)
         keep.extend([t_l, t_m, kx0, ky0, polar, spec_of_unit, src_order, src_2kz])
         return d
+
+    def check(self) -> None:
+        """Raise EuvError if a device wait of the plan's own calls gave up, an LU
+        met a zero pivot or the double-angle steps were clamped (synchronises
+        the current stream; clears the word)."""
+        _check_word(self.status, "Plan")
 
     def run_amp(self, desc: L.AmpDesc, spectra: torch.Tensor, ax: torch.Tensor) -> None:
         wb = L.lib().euv_amp_workspace_bytes(C.byref(desc))
@@ -229,6 +238,7 @@ class Plan:
                              self._f64(np.tile(kz2, (nc, 1))), keep)
         ax = torch.empty((nc, len(srcs), self.orders.n), dtype=torch.complex128, device=self.device)
         self.run_amp(desc, spec, ax)
+        self.check()
         return ax, srcs
 
     # ------------------------------------------------------------ Abbe
@@ -289,6 +299,7 @@ class Plan:
             b.run_plain()
         else:
             b.run()
+        b.check()
         return b.image.clone()
 
     # ------------------------------------------------------------ M3D
@@ -331,6 +342,7 @@ class Plan:
                              self._i32(np.tile(src_nn, (2, 1))), self._f64(np.tile(kz2, (2, 1))), keep)
         axn = torch.empty((2, ns, narrow.n), dtype=torch.complex128, device=self.device)
         self.run_amp(desc, spec, axn)
+        self.check()
         tb = dict(
             narrow=narrow, srcs=srcs, ns=ns,
             src_l=self._i32([s[0] for s in srcs]), src_m=self._i32([s[1] for s in srcs]),
@@ -367,6 +379,13 @@ class Plan:
                axp.data_ptr(), ayp.data_ptr(), _stream())
         self._last_keep = (ax_wide, fmask)
         return {"a0": a0, "ax": axp, "ay": ayp, "Ax": ax_wide, "srcs": srcs}
+
+
+def _check_word(word: torch.Tensor, where: str) -> None:
+    bits = int(word.item())
+    if bits:
+        word.zero_()
+        L.check_status(where, bits)
 
 
 class IntensityBatch:
@@ -409,8 +428,11 @@ class IntensityBatch:
         self.t_clip = plan._i32(clip)
         self.t_order = plan._i32(tb["order"][tab])
         self.t_kz2 = plan._f64(tb["kz2"][tab])
+        # device status word of this batch's ampS calls (EUV_STATUS_* bits)
+        self.status = torch.zeros(1, dtype=torch.int32, device=dev)
         self.desc = plan.amp_desc(plan.orders, plan._t_l, plan._t_m, self.t_kx0, self.t_ky0,
-                                  self.t_pol, self.t_clip, self.t_order, self.t_kz2, self.keep)
+                                  self.t_pol, self.t_clip, self.t_order, self.t_kz2, self.keep,
+                                  status=self.status)
         self.t_tab, self.t_img, self.t_ns = plan._i32(tab), plan._i32(img), plan._i32(tb["nsrc"][tab])
         self.inv_w = plan._f64([1.0 / plan.sdivsum] * (nc * npol))
         ad = L.AbbeDesc()
@@ -494,6 +516,11 @@ class IntensityBatch:
         for d, a, axp, wb in self._plain:
             L.call("euv_amp", C.byref(d), self.spec.data_ptr(), axp, w.data_ptr(), wb, _stream())
             L.call("euv_abbe", C.byref(a), axp, self.image.data_ptr(), _stream())
+
+    def check(self) -> None:
+        """Raise EuvError if the device status word of the batch's runs since
+        the last check has a bit set (synchronises the current stream)."""
+        _check_word(self.status, "IntensityBatch")
 
     def capture(self) -> None:
         """Capture run() into a CUDA graph (call run() once before, outside capture)."""

@@ -146,7 +146,7 @@ def main(argv=None) -> int:
             def fn():
                 L.call("euv_zgemm_tf32x3", n, n, n, L.c64(1, 0), None, A.data_ptr(), n, n * n,
                        B.data_ptr(), n, n * n, L.c64(0, 0), C.data_ptr(), n, n * n, L.c64(0, 0),
-                       b, None, 0, ws.data_ptr(), wb, s)
+                       b, None, 0, ws.data_ptr(), wb, None, s)
         else:
             def fn():
                 L.call("euv_zgemm", n, n, n, L.c64(1, 0), None, A.data_ptr(), n, n * n,

@@ -83,6 +83,7 @@ class Request:
     arrival: float            # seconds on the server clock
     image: Optional[np.ndarray] = None
     done: Optional[float] = None
+    error: Optional[str] = None   # set (and image None) when the device reported a failure
 
     @property
     def latency(self) -> Optional[float]:
@@ -137,6 +138,7 @@ class Executor:
             self.need = max(self.batch.spec_bytes, max(c[3] for c in self.batch._plain))
         self.hin = torch.zeros(tuple(self.batch.masks.shape), dtype=torch.uint8).pin_memory()
         self.hout = torch.empty(tuple(self.batch.image.shape), dtype=torch.float64).pin_memory()
+        self.hstat = torch.zeros(1, dtype=torch.int32).pin_memory()
         b = self.batch
         self.bytes = int(sum(t.numel() * t.element_size() for t in (b.masks, b.spec_raw, b.ax, b.image)))
         self.busy = False
@@ -151,6 +153,9 @@ class Executor:
             else:
                 self.batch.run(work)
             self.hout.copy_(self.batch.image, non_blocking=True)
+            # the batch's device status word travels with its image, then restarts at 0
+            self.hstat.copy_(self.batch.status, non_blocking=True)
+            self.batch.status.zero_()
             ev = torch.cuda.Event()
             ev.record(stream)
         return ev
@@ -230,6 +235,7 @@ class Server:
         t0 = time.perf_counter()
         batches = 0
         clips = 0
+        failed = 0
         while nxt < len(reqs) or inflight or any(pending.values()):
             now = time.perf_counter() - t0
             while nxt < len(reqs) and reqs[nxt].arrival <= now:
@@ -240,9 +246,12 @@ class Server:
                 if ev.query():
                     t = time.perf_counter() - t0
                     img = ex.hout.numpy()
+                    err = L.status_message(int(ex.hstat[0]))
                     for i, r in enumerate(rs):
-                        r.image = img[i].copy()
+                        r.image = None if err else img[i].copy()
+                        r.error = err
                         r.done = t
+                    failed += len(rs) if err else 0
                     ex.busy = False
                     self.arena.free(off)
                     free_slots.append(slot)
@@ -293,6 +302,7 @@ class Server:
             "arena_bytes": self.arena.size,
             "resident_bytes": self.resident_bytes,
             "waits_for_memory": self.waits_for_memory,
+            "failed": failed,
         }
 
 

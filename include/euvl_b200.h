@@ -39,6 +39,15 @@ extern "C" {
 #define EUV_ERR_CUDA 2
 #define EUV_ERR_WORKSPACE 3
 #define EUV_ERR_SINGULAR 4
+#define EUV_ERR_TIMEOUT 5  /* a bounded device wait expired (euv_wait_probe) */
+
+/* Bits of a caller-owned device status word (euv_amp_desc.d_status, the d_status
+ * argument of euv_zgemm_tf32x3 and euv_wait_probe).  The library only ORs bits
+ * in; the caller zeroes the word and reads it when the stream is idle (the
+ * reference checks none of these conditions, header.h:498,888,1529). */
+#define EUV_STATUS_TIMEOUT 1       /* a bounded device wait gave up: that call's results are incomplete */
+#define EUV_STATUS_STEPS_CLAMPED 2 /* a unit needed more double-angle steps than m_max */
+#define EUV_STATUS_SINGULAR 4      /* an LU met an exactly zero pivot */
 
 #define EUV_MAX_SLICES 32
 
@@ -121,6 +130,7 @@ typedef struct {
   int precision;         /* EUV_PREC_FP64 or EUV_PREC_MIXED */
   int m_max;             /* upper bound on double-angle steps; <= 0: derived */
   double k0_max;         /* bound on |kx0|, |ky0| over the units (<= 0: k) */
+  int* d_status;         /* optional device int: EUV_STATUS_* bits OR-ed in (NULL: none) */
 } euv_amp_desc;
 
 size_t euv_amp_workspace_bytes(const euv_amp_desc* desc);
@@ -218,13 +228,22 @@ int euv_zgemm(int m, int n, int k, euv_c64 alpha, const double* d_scale, const e
 /* The bulk product of EUV_PREC_MIXED: same contract as euv_zgemm, computed on
  * the tcgen05 tensor cores as TF32x3 (each FP64 operand split into two TF32
  * terms, three TF32 products per real product, FP32 accumulation; ~1e-6
- * relative error per product).  Needs a workspace for the split operands. */
+ * relative error per product).  Needs a workspace for the split operands.
+ * d_status (optional device int): EUV_STATUS_TIMEOUT is OR-ed in if one of the
+ * kernel's bounded waits (about 2 s) gave up. */
 size_t euv_zgemm_tf32x3_workspace_bytes(int m, int n, int k, int batch);
 int euv_zgemm_tf32x3(int m, int n, int k, euv_c64 alpha, const double* d_scale,
                      const euv_c64* d_a, int lda, long long stride_a, const euv_c64* d_b, int ldb,
                      long long stride_b, euv_c64 beta, euv_c64* d_c, int ldc, long long stride_c,
                      euv_c64 diag, int batch, const int* d_steps, int step, void* d_work,
-                     size_t work_bytes, void* stream);
+                     size_t work_bytes, int* d_status, void* stream);
+
+/* One device thread waits until *d_flag != 0, with the bounded spin that every
+ * device wait of the library uses (limit_ns, at most 2e9); on expiry it ORs
+ * EUV_STATUS_TIMEOUT into *d_status and returns.  No reference counterpart:
+ * it lets a caller check that an expired wait comes back as a status while
+ * the context stays usable. */
+int euv_wait_probe(const int* d_flag, long long limit_ns, int* d_status, void* stream);
 
 /* Batched LU with partial pivoting, in place (replaces the getrf branch of
  * matinv, header.h:1518-1529).  d_ipiv[b][j] (0-based row swapped with j);

@@ -57,3 +57,38 @@ def test_struct_sizes_match_c_layout():
     # natural C alignment of the descriptors (x86-64 ABI)
     assert C.sizeof(L.c64) == 16
     assert C.sizeof(L.Stack) == 6 * 16 + 6 * 8 + 8
+
+
+def test_wait_probe_rejects_bad_arguments(lib):
+    # validated before any launch, so this runs without a GPU
+    assert lib.euv_wait_probe(None, 1000, None, None) == L.EUV_ERR_BAD_ARG
+    assert lib.euv_wait_probe(None, -1, None, None) == L.EUV_ERR_BAD_ARG
+    assert b"euv_wait_probe" in lib.euv_last_error()
+
+
+def test_descriptor_layout_matches_the_header(tmp_path):
+    """sizeof / offsetof of every descriptor, from the C compiler, against the
+    ctypes mirrors."""
+    import subprocess
+    structs = {"euv_amp_desc": L.AmpDesc, "euv_abbe_desc": L.AbbeDesc, "euv_m3d_desc": L.M3dDesc,
+               "euv_stack": L.Stack}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "euvl_b200.h"', "int main(void) {"]
+    for cname, py in structs.items():
+        lines.append('printf("%s size %%zu\\n", sizeof(%s));' % (cname, cname))
+        for f, _ in py._fields_:
+            lines.append('printf("%s %s %%zu\\n", offsetof(%s, %s));' % (cname, f, cname, f))
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {}
+    for ln in out:
+        if ln.strip():
+            k1, k2, v = ln.split()
+            got[(k1, k2)] = int(v)
+    for cname, py in structs.items():
+        assert got[(cname, "size")] == C.sizeof(py), cname
+        for f, _ in py._fields_:
+            assert got[(cname, f)] == getattr(py, f).offset, (cname, f)

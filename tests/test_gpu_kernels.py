@@ -164,10 +164,12 @@ def test_zgemm_tf32x3(cuda, m, n, k, batch):
     dA, dB, dC = _t(_colmajor(A), cuda), _t(_colmajor(B), cuda), _t(_colmajor(Cm), cuda)
     wb = L.lib().euv_zgemm_tf32x3_workspace_bytes(m, n, k, batch)
     ws = torch.empty(wb, dtype=torch.uint8, device=cuda)
+    st = torch.zeros(1, dtype=torch.int32, device=cuda)
     L.call("euv_zgemm_tf32x3", m, n, k, L.c64.of(alpha), None, dA.data_ptr(), m, m * k,
            dB.data_ptr(), k, k * n, L.c64.of(beta), dC.data_ptr(), m, m * n, L.c64.of(diag), batch,
-           None, 0, ws.data_ptr(), wb, _stream())
+           None, 0, ws.data_ptr(), wb, st.data_ptr(), _stream())
     torch.cuda.synchronize()
+    assert st.item() == 0  # no bounded wait gave up
     got = _from_colmajor(dC.cpu().numpy(), m, n)
     ref = alpha * (A @ B) + beta * Cm
     for b in range(batch):
@@ -187,7 +189,7 @@ def test_zgemm_tf32x3_step_copy(cuda):
     ws = torch.empty(wb, dtype=torch.uint8, device=cuda)
     L.call("euv_zgemm_tf32x3", n, n, n, L.c64.of(1.0), None, dA.data_ptr(), n, n * n,
            dA.data_ptr(), n, n * n, L.c64.of(0), dC.data_ptr(), n, n * n, L.c64.of(0), batch,
-           steps.data_ptr(), 1, ws.data_ptr(), wb, _stream())
+           steps.data_ptr(), 1, ws.data_ptr(), wb, None, _stream())
     torch.cuda.synchronize()
     got = _from_colmajor(dC.cpu().numpy(), n, n)
     assert rel_err(got[0], A[0]) == 0.0
