@@ -35,7 +35,7 @@ EXPORTS = (
     "euv_abbe", "euv_m3d_fit",
     "euv_zgemm", "euv_zgemm_tf32x3_workspace_bytes", "euv_zgemm_tf32x3", "euv_lu_workspace_bytes", "euv_lu_factor", "euv_lu_solve",
     "euv_matfun_workspace_bytes", "euv_matfun_cs", "euv_matfun_cs_noalloc",
-    "euv_wait_probe",
+    "euv_wait_probe", "euv_linear_amp",
 )
 
 
@@ -109,6 +109,15 @@ class M3dDesc(C.Structure):
     ]
 
 
+class LinearDesc(C.Structure):
+    _fields_ = [
+        ("n_clips", C.c_int), ("n_src", C.c_int), ("ncut", C.c_int), ("lpx", C.c_int),
+        ("lpy", C.c_int), ("d_lp", P), ("d_mp", P), ("d_ls", P), ("d_ms", P),
+        ("k", C.c_double), ("dx", C.c_double), ("dy", C.c_double), ("kx0", C.c_double),
+        ("ky0", C.c_double), ("z0", C.c_double), ("amp_vc", c64), ("amp_ab", c64),
+    ]
+
+
 _lib: Optional[C.CDLL] = None
 
 
@@ -149,6 +158,8 @@ def _declare(lib: C.CDLL) -> None:
     lib.euv_matfun_cs_noalloc.restype = i
     lib.euv_matfun_cs_noalloc.argtypes = [i, P, P, P, P, i, i, P]
     lib.euv_wait_probe.restype = i
+    lib.euv_linear_amp.restype = i
+    lib.euv_linear_amp.argtypes = [C.POINTER(LinearDesc), P, P, P, P, P, P]
     lib.euv_wait_probe.argtypes = [P, ll, P, P]
 
 

@@ -2,6 +2,7 @@
 
   python -m euvlitho_b200.cli intensity   # int.out: ./mask.bin -> emint.csv
   python -m euvlitho_b200.cli m3d         # m3d.out: ./mask.bin -> inputxx.csv, inputlm.csv
+  python -m euvlitho_b200.cli linear      # linear.py: ./mask.bin + inputxx.csv -> intlinear.csv, intft.csv
 
 Both run the reference configuration (intensity.cpp:44-91, m3d.cpp:34-95) on
 the GPU; --preset picks another workload.
@@ -22,7 +23,8 @@ from .engine import Plan
 
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("what", choices=["intensity", "m3d"])
+    ap.add_argument("what", choices=["intensity", "m3d", "linear"])
+    ap.add_argument("--inputxx", default="./inputxx.csv", help="M3D parameters (linear)")
     ap.add_argument("--preset", default="reference")
     ap.add_argument("--mask", default="./mask.bin")
     ap.add_argument("--count", type=int, default=1, help="masks in the file (m3d ndata)")
@@ -33,7 +35,14 @@ def main(argv=None) -> int:
     t0 = time.time()
     plan = Plan(cfg, precision=a.precision, pols=(a.pol,))
     masks = torch.from_numpy(io.read_mask_bin(a.mask, cfg.ndivx, cfg.ndivy, a.count))
-    if a.what == "intensity":
+    if a.what == "linear":
+        p = io.read_inputxx(a.inputxx)
+        ax = io.expand_xinput(p["ax"], plan.xinput)
+        ay = io.expand_xinput(p["ay"], plan.xinput)
+        lin, ft = plan.linear(masks[:1], p["a0"][None], ax[None], ay[None])
+        io.write_image_full("intlinear.csv", lin[0].cpu().numpy())
+        io.write_image_full("intft.csv", ft[0].cpu().numpy())
+    elif a.what == "intensity":
         img = plan.intensity(masks[:1]).cpu().numpy()
         io.write_emint("emint.csv" if a.pol == "X" else "emintY.csv", img[0, 0])
     else:

@@ -67,6 +67,9 @@ class SimConfig:
     # absorber.  1 reproduces the revision that wrote the reference's golden
     # emint.csv / inputxx.csv, whose flip is one row off.
     yflip_offset: int = 0
+    # central obscuration of the pupil as a fraction of NA, used by the linear
+    # model's E-field (elitho/const.py co: 0.2 at NA 0.55, 0 at NA 0.33)
+    obscuration: float = 0.0
 
     # --- derived quantities (intensity.cpp:52-146) ---
     @property

@@ -112,6 +112,8 @@ class Plan:
         self._t_m = torch.tensor(mi, dtype=torch.int32, device=dev)
         self._abbe_tables = None
         self._m3d_tables = None
+        self._linear_tables = None
+        self._uniform = None
         self._batches: Dict[Tuple[int, int], "IntensityBatch"] = {}
         # device status word of the plan's own ampS calls (EUV_STATUS_* bits)
         self.status = torch.zeros(1, dtype=torch.int32, device=dev)
@@ -303,11 +305,14 @@ class Plan:
         return b.image.clone()
 
     # ------------------------------------------------------------ M3D
-    def m3d_tables(self):
-        if self._m3d_tables is not None:
-            return self._m3d_tables
+    def uniform_solves(self):
+        """Mask-independent narrow solves (m3d.cpp:214-238): Ax of the all-vacuum
+        and all-absorber masks on the narrow order set (ellipse, cut 1.5,
+        m3d.cpp:107-129) for the NA-circle source orders (cached)."""
+        if self._uniform is not None:
+            return self._uniform
         cfg = self.cfg
-        ln, mn = cfg.order_limits("ellipse", 1.5)  # m3d.cpp:107-129
+        ln, mn = cfg.order_limits("ellipse", 1.5)
         nli, nmi = T.order_set("ellipse", ln, mn)
         narrow = OrderSet("ellipse", ln, mn, nli, nmi)
         npos = T.order_positions(nli, nmi)
@@ -316,21 +321,11 @@ class Plan:
         src_nn = np.array([npos.get(s, -1) for s in srcs], np.int32)
         if np.any(src_nn < 0):
             raise ValueError("narrow order set misses a source order")
-        pair = np.full((self.ncut, ns), -1, np.int32)
-        for n in range(self.ncut):
-            lp, mp = int(self.linput[n]), int(self.minput[n])
-            for s, (ls, ms) in enumerate(srcs):
-                if T.in_na(cfg, ls + lp, ms + mp):
-                    o = self.pos.get((ls + lp, ms + mp))
-                    if o is None:
-                        raise ValueError("order set misses pupil order %s" % ((ls + lp, ms + mp),))
-                    pair[n, s] = o
-        # mask-independent narrow solves on the all-vacuum / all-absorber masks
         nb = self.mask_bytes()
         uni = torch.stack([torch.full((nb,), 255, dtype=torch.uint8),
                            torch.zeros(nb, dtype=torch.uint8)]).to(self.device)
         spec = self.spectra(uni.view(2, 1, nb), 2 * ln, 2 * mn)
-        o, kz2 = [], []
+        kz2 = []
         for (ls, ms) in srcs:
             kx = cfg.kx0 + ls * 2.0 * PI / cfg.dx
             ky = cfg.ky0 + ms * 2.0 * PI / cfg.dy
@@ -343,13 +338,33 @@ class Plan:
         axn = torch.empty((2, ns, narrow.n), dtype=torch.complex128, device=self.device)
         self.run_amp(desc, spec, axn)
         self.check()
+        self._uniform = dict(narrow=narrow, srcs=srcs, ns=ns, src_nn=src_nn,
+                             s_center=srcs.index((0, 0)), n00=npos[(0, 0)],
+                             ax_vc=axn[0].contiguous(), ax_ab=axn[1].contiguous(), keep=keep)
+        return self._uniform
+
+    def m3d_tables(self):
+        if self._m3d_tables is not None:
+            return self._m3d_tables
+        u = self.uniform_solves()
+        srcs = u["srcs"]
+        ns = u["ns"]
+        pair = np.full((self.ncut, ns), -1, np.int32)
+        for n in range(self.ncut):
+            lp, mp = int(self.linput[n]), int(self.minput[n])
+            for s, (ls, ms) in enumerate(srcs):
+                if T.in_na(self.cfg, ls + lp, ms + mp):
+                    o = self.pos.get((ls + lp, ms + mp))
+                    if o is None:
+                        raise ValueError("order set misses pupil order %s" % ((ls + lp, ms + mp),))
+                    pair[n, s] = o
         tb = dict(
-            narrow=narrow, srcs=srcs, ns=ns,
+            narrow=u["narrow"], srcs=srcs, ns=ns,
             src_l=self._i32([s[0] for s in srcs]), src_m=self._i32([s[1] for s in srcs]),
-            src_nn=self._i32(src_nn), s_center=srcs.index((0, 0)),
-            ax_vc=axn[0].contiguous(), ax_ab=axn[1].contiguous(),
+            src_nn=self._i32(u["src_nn"]), s_center=u["s_center"],
+            ax_vc=u["ax_vc"], ax_ab=u["ax_ab"],
             lin=self._i32(self.linput), min=self._i32(self.minput), xin=self._i32(self.xinput),
-            pair=self._i32(pair), keep=keep,
+            pair=self._i32(pair), keep=u["keep"],
         )
         self._m3d_tables = tb
         return tb
@@ -379,6 +394,77 @@ class Plan:
                axp.data_ptr(), ayp.data_ptr(), _stream())
         self._last_keep = (ax_wide, fmask)
         return {"a0": a0, "ax": axp, "ay": ayp, "Ax": ax_wide, "srcs": srcs}
+
+
+    # ------------------------------------------------------------ linear model
+    def linear_tables(self, mesh_deg: float = 0.2):
+        """Resident tables of the linear model (linear.py:47-172): source grid,
+        E-field factors and identity pupil indices for the fused Abbe kernel,
+        and the specular amplitudes of the all-vacuum / all-absorber masks
+        (the narrow solves of the M3D tables)."""
+        tb = self._linear_tables
+        if tb is not None and tb["mesh"] == mesh_deg:
+            return tb
+        cfg = self.cfg
+        dsx, dsy = T.linear_sources(cfg, mesh_deg)
+        if len(dsx) == 0:
+            raise ValueError("the linear model's source grid is empty (mesh %g deg)" % mesh_deg)
+        coef, nidx = T.linear_abbe_table(cfg, dsx, dsy, self.linput, self.minput)
+        u = self.uniform_solves()
+        sc, n00 = u["s_center"], u["n00"]
+        vc = complex(u["ax_vc"][sc, n00].item())
+        ab = complex(u["ax_ab"][sc, n00].item())
+        tb = dict(mesh=mesh_deg, n_src=len(dsx), dsx=dsx, dsy=dsy,
+                  coef=self._c128(coef[None]), nidx=self._i32(nidx[None]),
+                  ls=self._f64(dsx * cfg.dx / (2.0 * PI)), ms=self._f64(dsy * cfg.dy / (2.0 * PI)),
+                  lp=self._i32(self.linput), mp=self._i32(self.minput),
+                  row_start=self._i32(T.row_starts(self.linput, cfg.lpmaxX)),
+                  amp_vc=vc, amp_ab=ab)
+        self._linear_tables = tb
+        return tb
+
+    def linear(self, masks, a0, ax, ay, mesh_deg: float = 0.2, thin: bool = True):
+        """Linear Abbe images from the M3D parameters (linear.py:45-188).
+
+        ``a0``, ``ax``, ``ay``: [clips, ncut] complex, one value per pupil point
+        (``Plan.m3d`` returns them so; ``io.read_inputxx`` + ``expand_xinput``
+        for a file).  Returns (intlinear [clips, XDIV, YDIV], intft or None):
+        the M3D-corrected image and, with ``thin``, the thin-mask one."""
+        cfg = self.cfg
+        tb = self.linear_tables(mesh_deg)
+        m = self.as_mask_tensor(masks)
+        nc, S, ncut = m.shape[0], tb["n_src"], self.ncut
+        par = []
+        for v in (a0, ax, ay):
+            t = torch.as_tensor(v).to(self.device, torch.complex128).reshape(nc, ncut).contiguous()
+            par.append(t)
+        fvac = self.spectra(m[:, :1], cfg.lpmaxX, cfg.lpmaxY, select_vacuum=1, per_slice=False)
+        d = L.LinearDesc()
+        d.n_clips, d.n_src, d.ncut, d.lpx, d.lpy = nc, S, ncut, cfg.lpmaxX, cfg.lpmaxY
+        d.d_lp, d.d_mp, d.d_ls, d.d_ms = _ptr(tb["lp"]), _ptr(tb["mp"]), _ptr(tb["ls"]), _ptr(tb["ms"])
+        d.k, d.dx, d.dy, d.kx0, d.ky0, d.z0 = cfg.k, cfg.dx, cfg.dy, cfg.kx0, cfg.ky0, cfg.z0
+        d.amp_vc, d.amp_ab = L.c64.of(tb["amp_vc"]), L.c64.of(tb["amp_ab"])
+        amp = torch.empty((nc, S, ncut), dtype=torch.complex128, device=self.device)
+        t_tab = self._i32([0] * nc)
+        t_img = self._i32(range(nc))
+        t_ns = self._i32([S] * nc)
+        inv_w = self._f64([1.0 / S] * nc)
+        ad = L.AbbeDesc()
+        ad.xdiv, ad.ydiv, ad.lpx, ad.lpy = cfg.xdiv, cfg.ydiv, cfg.lpmaxX, cfg.lpmaxY
+        ad.ncut, ad.n_units, ad.n_src, ad.n_order = ncut, nc, S, ncut
+        ad.d_coef, ad.d_nidx = _ptr(tb["coef"]), _ptr(tb["nidx"])
+        ad.d_px, ad.d_py, ad.d_row_start = _ptr(tb["lp"]), _ptr(tb["mp"]), _ptr(tb["row_start"])
+        ad.d_tab_of_unit, ad.d_img_of_unit, ad.d_nsrc_of_unit = _ptr(t_tab), _ptr(t_img), _ptr(t_ns)
+        ad.n_images, ad.d_inv_weight = nc, _ptr(inv_w)
+        out = []
+        for with_m3d in ((True, False) if thin else (True,)):
+            ptrs = [t.data_ptr() for t in par] if with_m3d else [None, None, None]
+            L.call("euv_linear_amp", C.byref(d), fvac.data_ptr(), *ptrs, amp.data_ptr(), _stream())
+            img = torch.zeros((nc, cfg.xdiv, cfg.ydiv), dtype=torch.float64, device=self.device)
+            L.call("euv_abbe", C.byref(ad), amp.data_ptr(), img.data_ptr(), _stream())
+            out.append(img)
+        self._last_keep = (fvac, amp, t_tab, t_img, t_ns, inv_w, par)
+        return out[0], (out[1] if thin else None)
 
 
 def _check_word(word: torch.Tensor, where: str) -> None:

@@ -71,6 +71,25 @@ def read_inputxx(path_or_file):
     return {"a0": rows[0] + 1j * rows[1], "ax": rows[2] + 1j * rows[3], "ay": rows[4] + 1j * rows[5]}
 
 
+def expand_xinput(values, xinput) -> np.ndarray:
+    """Slopes stored for the xinput points only (inputxx.csv rows 3-6) -> one
+    value per pupil point, zero elsewhere."""
+    out = np.zeros(len(xinput), np.complex128)
+    out[np.asarray(xinput) == 1] = values
+    return out
+
+
+def write_image_full(path: str, image: np.ndarray) -> None:
+    """linear.py's intlinear.csv / intft.csv layout (linear.py:245-258): row j
+    holds I[i][XDIV-1-j] for i < XDIV, each value at full precision followed by
+    a comma."""
+    n = image.shape[0]
+    with open(path, "w") as fh:
+        for j in range(n):
+            fh.write("".join("%r," % float(image[i, n - 1 - j]) for i in range(n)))
+            fh.write("\n")
+
+
 def write_inputlm(path: str, linput, minput, xinput) -> None:
     with open(path, "w") as fh:
         for l, m, x in zip(linput, minput, xinput):

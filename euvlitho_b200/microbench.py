@@ -4,6 +4,7 @@
   python -m euvlitho_b200.microbench zgemm  --n 961 --batch 4
   python -m euvlitho_b200.microbench lu     --n 961 --batch 24 --nrhs 96
   python -m euvlitho_b200.microbench step   --precision mixed --clips 4
+  python -m euvlitho_b200.microbench linear --preset reference --clips 1
   python -m euvlitho_b200.microbench summarize launches.csv
 
 Times each library entry point with CUDA events on the launching stream after
@@ -14,6 +15,8 @@ polarisations = 6 units per clip) untimed, then `--reps` steps between
 cudaProfilerStart/Stop, so that `ncu --profile-from-start off` lists exactly
 those steps' launches; `--compare` adds the FP64 form's image and the mixed
 form's intensity error against it.
+`linear` times the linear Abbe model (M3D-parameter amplitudes + two fused
+Abbe images per clip) with tables resident, on seeded masks and parameters.
 `summarize` folds an ncu `--csv` launch list of gpu__time_duration.sum into
 launches, total time and share per kernel.
 """
@@ -96,6 +99,29 @@ def _step(a) -> dict:
     return out
 
 
+def _linear(a) -> dict:
+    import numpy as np
+    from . import masks as MK
+    from .config import preset
+    from .engine import Plan
+    cfg = preset(a.preset)
+    plan = Plan(cfg, device=torch.device("cuda"))
+    tb = plan.linear_tables()
+    rng = np.random.default_rng(0)
+    par = [torch.from_numpy((rng.standard_normal((a.clips, plan.ncut))
+                             + 1j * rng.standard_normal((a.clips, plan.ncut))) * 1e-3).cuda()
+           for _ in range(3)]
+    bits = torch.from_numpy(MK.batch(cfg.ndivx, cfg.ndivy, range(a.clips))).cuda()
+    ms = _time(lambda: plan.linear(bits, *par), a.reps)
+    S, ncut, bx = tb["n_src"], plan.ncut, 2 * cfg.lpmaxX + 1
+    by = 2 * cfg.lpmaxY + 1
+    # Abbe per image: per source, 3 components x (stage y: YDIV x ncut + stage x: XDIV x YDIV x bx)
+    flop = 2 * a.clips * S * 3 * 8.0 * (cfg.ydiv * ncut + cfg.xdiv * cfg.ydiv * bx)
+    return {"preset": a.preset, "clips": a.clips, "sources": S, "ncut": ncut, "pupil_box": [bx, by],
+            "ms_per_call": ms, "clips_per_s": a.clips / (ms / 1e3),
+            "abbe_fp64_tflops": flop / (ms / 1e3) / 1e12}
+
+
 def _time(fn, reps: int) -> float:
     for _ in range(3):
         fn()
@@ -113,7 +139,7 @@ def _time(fn, reps: int) -> float:
 
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("kernel", choices=["tf32x3", "zgemm", "lu", "step", "summarize"])
+    ap.add_argument("kernel", choices=["tf32x3", "zgemm", "lu", "step", "linear", "summarize"])
     ap.add_argument("csv", nargs="?", help="ncu --csv launch list (summarize)")
     ap.add_argument("--n", type=int, default=961)
     ap.add_argument("--batch", type=int, default=4)
@@ -130,6 +156,9 @@ def main(argv=None) -> int:
         return 0
     if a.kernel == "step":
         print(json.dumps(_step(a)))
+        return 0
+    if a.kernel == "linear":
+        print(json.dumps(_linear(a)))
         return 0
     n, b = a.n, a.batch
     s = torch.cuda.current_stream().cuda_stream

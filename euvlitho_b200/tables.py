@@ -217,3 +217,49 @@ def row_starts(linput: np.ndarray, lpx: int) -> np.ndarray:
     if np.any(np.diff(linput) < 0):
         raise ValueError("pupil points must be l-major")
     return np.searchsorted(linput, np.arange(-lpx, lpx + 2), side="left").astype(np.int32)
+
+
+# ----------------------------------------------------------- linear model
+def linear_sources(cfg: SimConfig, mesh_deg: float = 0.2) -> Tuple[np.ndarray, np.ndarray]:
+    """Source shifts (dsx, dsy) of the linear model (linear.py:47-96): a square
+    grid of step k * mesh (radians) in the mask-side source plane, l outer and
+    m inner, kept where the illumination holds at (MX dsx, MY dsy)."""
+    k, NA = cfg.k, cfg.na
+    kmesh = k * mesh_deg * (PI / 180.0)
+    l0max = int(k * NA / cfg.mx * cfg.sigma1 / kmesh) + 1
+    m0max = int(k * NA / cfg.my * cfg.sigma1 / kmesh) + 1
+    l, m = np.meshgrid(np.arange(-l0max, l0max + 1), np.arange(-m0max, m0max + 1), indexing="ij")
+    skx, sky = (l * kmesh).ravel(), (m * kmesh).ravel()
+    xo, yo = skx * cfg.mx, sky * cfg.my
+    r = np.sqrt(xo * xo + yo * yo)
+    r1, r2 = k * NA * cfg.sigma1, k * NA * cfg.sigma2
+    t = np.tan(PI * cfg.openangle / 180.0 / 2.0)
+    ring = (r2 <= r) & (r <= r1)
+    ok = {0: xo * xo + yo * yo <= r1 * r1, 1: ring,
+          2: ring & (np.abs(yo) <= np.abs(xo) * t),
+          3: ring & (np.abs(xo) <= np.abs(yo) * t)}[int(cfg.illum_type)]
+    return skx[ok], sky[ok]
+
+
+def linear_abbe_table(cfg: SimConfig, dsx, dsy, linput, minput):
+    """E-field factors of the linear model for the fused Abbe kernel:
+    coef[s][i][3] = i k R(:, 0) phase / sqrt(k^2 - (kx0 + dsx_s)^2) and the
+    identity index nidx[s][i] = i (-1 where the pupil point is outside
+    obscuration <= |p| / (NA k) <= 1), X polarisation, following
+    elitho/electro_field.py:45-76 and linear.py:11-43 (phase with z0 and the
+    defocus cfg.z)."""
+    k, dx, dy, MX, MY, NA = cfg.k, cfg.dx, cfg.dy, cfg.mx, cfg.my, cfg.na
+    kx0, ky0, z0, z = cfg.kx0, cfg.ky0, cfg.z0, float(cfg.z)
+    dsx = np.asarray(dsx, np.float64)[:, None]
+    dsy = np.asarray(dsy, np.float64)[:, None]
+    kxn = dsx + 2.0 * PI * np.asarray(linput, np.float64)[None, :] / dx
+    kyn = dsy + 2.0 * PI * np.asarray(minput, np.float64)[None, :] / dy
+    p2 = MX * MX * kxn * kxn + MY * MY * kyn * kyn
+    ok = (p2 <= (NA * k) ** 2) & (p2 >= (NA * k * cfg.obscuration) ** 2)
+    R = rotate(k, MX, MY, kxn, kyn, kx0, ky0)[..., 0]  # [S, ncut, 3]
+    phase = np.exp(1j * ((kxn + kx0) ** 2 + (kyn + ky0) ** 2) / (2.0 * k) * z0
+                   + 1j * p2 / (2.0 * k) * z)
+    f = 1j * k / np.sqrt(k * k - (kx0 + dsx) ** 2)
+    coef = np.where(ok[..., None], (f * phase)[..., None] * R, 0.0).astype(np.complex128)
+    nidx = np.where(ok, np.arange(len(linput), dtype=np.int32)[None, :], -1).astype(np.int32)
+    return coef, nidx

@@ -138,6 +138,34 @@ int euv_amp(const euv_amp_desc* desc, const euv_c64* d_spectra, euv_c64* d_ax, v
             size_t work_bytes, void* stream);
 
 /* ------------------------------------------------------------------------ */
+/* Linear Abbe model from M3D parameters: replaces the amplitude loop of
+ * cnn/intensity/linear/linear.py:120-172 (its image loop, linear.py:11-43, is
+ * euv_abbe with identity pupil tables, see below).  For clip c, source s of the
+ * linear model's source grid (shifts dsx, dsy, linear.py:47-96) and pupil
+ * point i (orders lp, mp):
+ *   famp(c,i)  = (ab delta(lp,mp) + (vc - ab) F_c(lp,mp)) phX(lp) phY(mp) / (vc/|vc|),
+ *   phX(lp)    = exp(-i (kx0 kxp + kxp^2/2) z0 / k),  kxp = 2 pi lp / dx (y alike),
+ *   A[c][s][i] = famp(c,i) + a0[c][i] + ax[c][i] (ls_s + lp/2) + ay[c][i] (ms_s + mp/2),
+ * ls_s = dsx_s dx / (2 pi), ms_s = dsy_s dy / (2 pi).  d_a0 == NULL gives the
+ * thin-mask (Kirchhoff) amplitude famp (linear.py's intft).  F_c is the
+ * vacuum-indicator spectrum of clip c (euv_mask_spectrum, select_vacuum = 1,
+ * lh = lpx, mh = lpy).  a0, ax, ay: [c][ncut], ax = ay = 0 where the M3D fit
+ * has no slope.  Output d_amp[c][s][i] feeds euv_abbe as its d_ax with
+ * n_order = ncut, d_nidx[s][i] = i (-1 outside the pupil) and coefficients
+ * i k R(:,0) phase / sqrt(k^2 - (kx0+dsx_s)^2). */
+typedef struct {
+  int n_clips, n_src, ncut, lpx, lpy;
+  const int* d_lp;         /* [ncut] pupil orders */
+  const int* d_mp;
+  const double* d_ls;      /* [n_src] source shifts in orders */
+  const double* d_ms;
+  double k, dx, dy, kx0, ky0, z0;
+  euv_c64 amp_vc, amp_ab;  /* specular amplitudes of the all-vacuum / all-absorber mask */
+} euv_linear_desc;
+int euv_linear_amp(const euv_linear_desc* desc, const euv_c64* d_fvac, const euv_c64* d_a0,
+                   const euv_c64* d_ax, const euv_c64* d_ay, euv_c64* d_amp, void* stream);
+
+/* ------------------------------------------------------------------------ */
 /* Fused Abbe imaging: replaces the per-source loop of intensity.cpp:248-408
  * (E-field through rotate(), pupil phase and defocus, scatter, three cuFFT Z2Z
  * inverse transforms, |Ex|^2+|Ey|^2+|Ez|^2, sum over sources / SDIVSUM) with one

@@ -110,6 +110,9 @@ class SimConfig:
     # 0; rows outside the mask are absorber).  1 reproduces the revision that
     # wrote the golden emint.csv / inputxx.csv.
     yflip_offset: int = 0
+    # central obscuration of the pupil as a fraction of NA, used by the linear
+    # model's E-field (elitho/const.py co: 0.2 at NA 0.55, 0 at NA 0.33)
+    obscuration: float = 0.0
 
     @property
     def dx(self) -> float:
@@ -616,6 +619,32 @@ def rotate(k, MX, MY, px, py, sx0, sy0) -> np.ndarray:
     return np.outer(esp, es[:2]) + np.outer(emp, em[:2])
 
 
+def rotate_many(k, MX, MY, px, py, sx0, sy0) -> np.ndarray:
+    """``rotate`` for arrays of pupil coordinates px, py: returns [n, 3, 2]."""
+    px = np.asarray(px, np.float64)
+    py = np.asarray(py, np.float64)
+    n = px.shape[0]
+    s0 = np.broadcast_to(np.array([sx0, sy0, -np.sqrt(k * k - sx0 * sx0 - sy0 * sy0)]), (n, 3))
+    p = np.stack([px, py, np.zeros(n)], -1)
+    with np.errstate(invalid="ignore"):
+        pp = np.stack([MX * px, MY * py, -np.sqrt(k * k - (MX * px) ** 2 - (MY * py) ** 2)], -1)
+    ez = np.broadcast_to(np.array([0.0, 0.0, 1.0]), (n, 3))
+    nrm = lambda v: v / np.linalg.norm(v, axis=-1, keepdims=True)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        es1 = nrm(np.cross(p, s0))
+        esp1 = nrm(np.cross(pp, ez))
+        em1 = np.cross(es1, nrm(p + s0))
+        emp1 = np.cross(esp1, pp) / k
+        es2 = nrm(np.cross(ez, s0))
+        esp2 = -es2
+        em2 = np.cross(es2, s0) / k
+        emp2 = np.cross(esp2, -ez)
+    big = ((px * px + py * py) > 0.00001)[:, None]
+    es, esp = np.where(big, es1, es2), np.where(big, esp1, esp2)
+    em, emp = np.where(big, em1, em2), np.where(big, emp1, emp2)
+    return esp[:, :, None] * es[:, None, :2] + emp[:, :, None] * em[:, None, :2]
+
+
 def abbe_family_fields(cfg: SimConfig, polar, Ax, lidx, midx, nsx, nsy, ndivs, pts,
                        linput, minput, z):
     """Pupil-grid fields of one family's source points (intensity.cpp:248-366).
@@ -819,6 +848,108 @@ def m3d(cfg: SimConfig, mask2d, polar="X", Ax_wide=None):
     sel = xinput == 1
     return {"a0": a0, "ax": ax[sel], "ay": ay[sel], "linput": linput, "minput": minput,
             "xinput": xinput, "Ax": Ax, "vcxx": vcxx, "abxx": abxx}
+
+
+# --------------------------------------------------------------------------
+# Linear Abbe model from the M3D parameters (cnn/intensity/linear/linear.py)
+# --------------------------------------------------------------------------
+def linear_sources(cfg: SimConfig, mesh_deg: float = 0.2):
+    """Source points of the linear model (linear.py:47-96): a square grid of
+    step kmesh = k * mesh (radians) in the mask-side source plane, l outer and
+    m inner, kept where the illumination holds at (MX skx, MY sky).  Returns
+    the shifts dsx, dsy (rad/nm) in that order."""
+    k, NA = cfg.k, cfg.na
+    kmesh = k * mesh_deg * (PI / 180.0)
+    l0max = int(k * NA / cfg.mx * cfg.sigma1 / kmesh) + 1
+    m0max = int(k * NA / cfg.my * cfg.sigma1 / kmesh) + 1
+    r1, r2 = k * NA * cfg.sigma1, k * NA * cfg.sigma2
+    t = np.tan(PI * cfg.openangle / 180.0 / 2.0)
+    dsx, dsy = [], []
+    for l in range(-l0max, l0max + 1):
+        for m in range(-m0max, m0max + 1):
+            skx, sky = l * kmesh, m * kmesh
+            xo, yo = skx * cfg.mx, sky * cfg.my
+            r = np.sqrt(xo * xo + yo * yo)
+            if cfg.illum_type == 0:
+                ok = xo * xo + yo * yo <= r1 * r1
+            elif cfg.illum_type == 1:
+                ok = r2 <= r <= r1
+            elif cfg.illum_type == 2:
+                ok = r2 <= r <= r1 and abs(yo) <= abs(xo) * t
+            else:
+                ok = r2 <= r <= r1 and abs(xo) <= abs(yo) * t
+            if ok:
+                dsx.append(skx)
+                dsy.append(sky)
+    return np.array(dsx), np.array(dsy)
+
+
+def linear_amplitudes(cfg: SimConfig, mask2d, a0, ax, ay, ampvc, ampab, dsx, dsy,
+                      linput, minput):
+    """Per source s and pupil point i, without the 1/sqrt(k^2 - kx^2) factor
+    (linear.py:120-172): the thin-mask amplitude
+        famp = (ab delta + (vc - ab) F_vac) phaseX phaseY / phase0
+    and the linear one  famp + a0 + ax (ls + lp/2) + ay (ms + mp/2)  with
+    ls = dsx / (2 pi / dx).  a0, ax, ay: one value per pupil point (ax, ay zero
+    where the fit has no slope).  Returns (A_linear, A_thin), [S][ncut]."""
+    k, dx, dy, z0 = cfg.k, cfg.dx, cfg.dy, cfg.z0
+    lpx, lpy = cfg.lpmaxX, cfg.lpmaxY
+    fvac = thin_mask_spectrum(mask2d, cfg)
+    lp = np.asarray(linput, np.float64)
+    mp = np.asarray(minput, np.float64)
+    f = (ampvc - ampab) * fvac[np.asarray(linput) + lpx, np.asarray(minput) + lpy]
+    f = f + np.where((lp == 0) & (mp == 0), ampab, 0.0)
+    kxp = 2.0 * PI * lp / dx
+    kyp = 2.0 * PI * mp / dy
+    ph = np.exp(-1j * (cfg.kx0 * kxp + kxp * kxp / 2.0) / k * z0) * \
+        np.exp(-1j * (cfg.ky0 * kyp + kyp * kyp / 2.0) / k * z0)
+    famp = f * ph / (ampvc / abs(ampvc))
+    ls = np.asarray(dsx)[:, None] / (2.0 * PI / dx)
+    ms = np.asarray(dsy)[:, None] / (2.0 * PI / dy)
+    alin = famp[None, :] + np.asarray(a0)[None, :] + np.asarray(ax)[None, :] * (ls + lp / 2.0) + \
+        np.asarray(ay)[None, :] * (ms + mp / 2.0)
+    return alin, np.broadcast_to(famp, alin.shape)
+
+
+def linear_image(cfg: SimConfig, amp, dsx, dsy, linput, minput, z: float = 0.0,
+                 obscuration: float = 0.0) -> np.ndarray:
+    """Abbe image of per-(source, pupil point) amplitudes on the linear model's
+    source grid (linear.py:11-43 with the high-NA E-field of
+    elitho/electro_field.py:45-76, X polarisation): E = i k R(:, 0) A /
+    sqrt(k^2 - kx^2) with kx = kx0 + dsx, zero outside obscuration <= |p|/(NA k)
+    <= 1; phase, scatter, unnormalised inverse DFT, |E|^2 summed over sources
+    and divided by their count.  Returns I[x][y]."""
+    k, dx, dy = cfg.k, cfg.dx, cfg.dy
+    MX, MY, NA = cfg.mx, cfg.my, cfg.na
+    kx0, ky0, z0 = cfg.kx0, cfg.ky0, cfg.z0
+    XD, YD = cfg.xdiv, cfg.ydiv
+    S = len(dsx)
+    lin = np.asarray(linput, np.int64)
+    mn = np.asarray(minput, np.int64)
+    isum = np.zeros((XD, YD))
+    for s in range(S):
+        kx = kx0 + dsx[s]
+        kxn = dsx[s] + 2.0 * PI * lin / dx
+        kyn = dsy[s] + 2.0 * PI * mn / dy
+        p2 = MX * MX * kxn * kxn + MY * MY * kyn * kyn
+        ok = np.nonzero((p2 <= (NA * k) ** 2) & (p2 >= (NA * k * obscuration) ** 2))[0]
+        F = np.zeros((3, XD, YD), np.complex128)
+        R = rotate_many(k, MX, MY, kxn[ok], kyn[ok], kx0, ky0)[:, :, 0]  # [n_ok, 3]
+        phase = np.exp(1j * ((kxn[ok] + kx0) ** 2 + (kyn[ok] + ky0) ** 2) / (2.0 * k) * z0
+                       + 1j * p2[ok] / (2.0 * k) * z)
+        E = 1j * k * R * (amp[s, ok] * phase / np.sqrt(k * k - kx * kx))[:, None]
+        F[:, lin[ok] % XD, mn[ok] % YD] = E.T
+        f = np.fft.ifft2(F, axes=(1, 2)) * (XD * YD)
+        isum += np.sum(f.real ** 2 + f.imag ** 2, axis=0) / S
+    return isum
+
+
+def expand_xinput(values, xinput):
+    """Slopes stored for the xinput points only (inputxx.csv rows 3-6) -> one
+    value per pupil point, zero elsewhere."""
+    out = np.zeros(len(xinput), np.complex128)
+    out[np.asarray(xinput) == 1] = values
+    return out
 
 
 def write_inputxx(path: str, res) -> None:

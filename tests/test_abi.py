@@ -51,6 +51,8 @@ def test_invalid_descriptors_are_rejected(lib):
     assert lib.euv_lu_factor(-1, None, 1, 0, None, None, 1, None) == L.EUV_ERR_BAD_ARG
     assert lib.euv_matfun_cs(0, None, None, None, None, 1, 4, 0, None, 0, None) == L.EUV_ERR_BAD_ARG
     assert lib.euv_mask_spectrum(None, 1, 8, 8, 8, 8, 1, 1, 0, 0, None, None, 0, None) == L.EUV_ERR_BAD_ARG
+    ld = L.LinearDesc()
+    assert lib.euv_linear_amp(C.byref(ld), None, None, None, None, None, None) == L.EUV_ERR_BAD_ARG
 
 
 def test_struct_sizes_match_c_layout():
@@ -71,7 +73,7 @@ def test_descriptor_layout_matches_the_header(tmp_path):
     ctypes mirrors."""
     import subprocess
     structs = {"euv_amp_desc": L.AmpDesc, "euv_abbe_desc": L.AbbeDesc, "euv_m3d_desc": L.M3dDesc,
-               "euv_stack": L.Stack}
+               "euv_stack": L.Stack, "euv_linear_desc": L.LinearDesc}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "euvl_b200.h"', "int main(void) {"]
     for cname, py in structs.items():
         lines.append('printf("%s size %%zu\\n", sizeof(%s));' % (cname, cname))
