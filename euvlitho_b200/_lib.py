@@ -35,7 +35,7 @@ EXPORTS = (
     "euv_abbe", "euv_m3d_fit",
     "euv_zgemm", "euv_zgemm_tf32x3_workspace_bytes", "euv_zgemm_tf32x3", "euv_lu_workspace_bytes", "euv_lu_factor", "euv_lu_solve",
     "euv_matfun_workspace_bytes", "euv_matfun_cs", "euv_matfun_cs_noalloc",
-    "euv_wait_probe", "euv_linear_amp",
+    "euv_wait_probe", "euv_linear_amp", "euv_mask_raster_workspace_bytes", "euv_mask_raster",
 )
 
 
@@ -159,6 +159,10 @@ def _declare(lib: C.CDLL) -> None:
     lib.euv_matfun_cs_noalloc.argtypes = [i, P, P, P, P, i, i, P]
     lib.euv_wait_probe.restype = i
     lib.euv_linear_amp.restype = i
+    lib.euv_mask_raster_workspace_bytes.restype = sz
+    lib.euv_mask_raster_workspace_bytes.argtypes = [i, i, i]
+    lib.euv_mask_raster.restype = i
+    lib.euv_mask_raster.argtypes = [i, i, i, i, P, i, P, P, P, sz, P]
     lib.euv_linear_amp.argtypes = [C.POINTER(LinearDesc), P, P, P, P, P, P]
     lib.euv_wait_probe.argtypes = [P, ll, P, P]
 

@@ -3,6 +3,7 @@
   python -m euvlitho_b200.cli intensity   # int.out: ./mask.bin -> emint.csv
   python -m euvlitho_b200.cli m3d         # m3d.out: ./mask.bin -> inputxx.csv, inputlm.csv
   python -m euvlitho_b200.cli linear      # linear.py: ./mask.bin + inputxx.csv -> intlinear.csv, intft.csv
+  python -m euvlitho_b200.cli maskgen     # mask.out: mask.bin (--count masks) + maskimage.csv
 
 Both run the reference configuration (intensity.cpp:44-91, m3d.cpp:34-95) on
 the GPU; --preset picks another workload.
@@ -23,7 +24,8 @@ from .engine import Plan
 
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("what", choices=["intensity", "m3d", "linear"])
+    ap.add_argument("what", choices=["intensity", "m3d", "linear", "maskgen"])
+    ap.add_argument("--seed", type=int, default=1, help="srand seed (maskgen; 1 = the reference's)")
     ap.add_argument("--inputxx", default="./inputxx.csv", help="M3D parameters (linear)")
     ap.add_argument("--preset", default="reference")
     ap.add_argument("--mask", default="./mask.bin")
@@ -33,6 +35,17 @@ def main(argv=None) -> int:
     a = ap.parse_args(argv)
     cfg = preset(a.preset)
     t0 = time.time()
+    if a.what == "maskgen":
+        from . import masks as MK
+        bits = MK.vbf_batch(a.count, cfg.ndivx, cfg.ndivy, seed=a.seed).cpu().numpy()
+        bits[:, 0].tofile("mask.bin")                    # mask.cpp:41-48
+        first = MK.unpack(bits[0, 0], cfg.ndivx, cfg.ndivy)
+        with open("maskimage.csv", "w") as fh:           # mask.cpp:49-59
+            for row in first:
+                fh.write("".join("%d," % v for v in row))
+                fh.write("\n")
+        print("elapsed time (s) %.3f" % (time.time() - t0))
+        return 0
     plan = Plan(cfg, precision=a.precision, pols=(a.pol,))
     masks = torch.from_numpy(io.read_mask_bin(a.mask, cfg.ndivx, cfg.ndivy, a.count))
     if a.what == "linear":

@@ -5,6 +5,7 @@
   python -m euvlitho_b200.microbench lu     --n 961 --batch 24 --nrhs 96
   python -m euvlitho_b200.microbench step   --precision mixed --clips 4
   python -m euvlitho_b200.microbench linear --preset reference --clips 1
+  python -m euvlitho_b200.microbench raster --clips 64 --slices 8
   python -m euvlitho_b200.microbench summarize launches.csv
 
 Times each library entry point with CUDA events on the launching stream after
@@ -17,6 +18,8 @@ those steps' launches; `--compare` adds the FP64 form's image and the mixed
 form's intensity error against it.
 `linear` times the linear Abbe model (M3D-parameter amplitudes + two fused
 Abbe images per clip) with tables resident, on seeded masks and parameters.
+`raster` times the device mask rasteriser on the reference generator's
+2048^2 masks (layouts drawn on the host beforehand), with sidewall slices.
 `summarize` folds an ncu `--csv` launch list of gpu__time_duration.sum into
 launches, total time and share per kernel.
 """
@@ -122,6 +125,21 @@ def _linear(a) -> dict:
             "abbe_fp64_tflops": flop / (ms / 1e3) / 1e12}
 
 
+def _raster(a) -> dict:
+    from . import masks as MK
+    n, nx = a.clips, 2048
+    r = MK.LibcRand(1)
+    rects = [MK.vbf_rectangles(nx, nx, r) for _ in range(n)]
+    radii = MK.sidewall_erosion(a.slices, 60.0 / a.slices)
+    out = torch.empty((n, a.slices, nx * nx // 8), dtype=torch.uint8, device="cuda")
+    ms = _time(lambda: MK.rasterize(rects, nx, nx, radii, out=out), a.reps)
+    steps = max(radii)
+    # bytes per mask: fill + paint (~1 B/pixel each), erosion 2 B/pixel per step, pack 1 B/pixel + bits
+    moved = n * nx * nx * (2 + 2 * steps + a.slices * (1 + 1.0 / 8))
+    return {"masks": n, "slices": a.slices, "erosion_steps": steps, "ms_per_call": ms,
+            "masks_per_s": n / (ms / 1e3), "gb_per_s_algorithmic": moved / (ms / 1e3) / 1e9}
+
+
 def _time(fn, reps: int) -> float:
     for _ in range(3):
         fn()
@@ -139,7 +157,9 @@ def _time(fn, reps: int) -> float:
 
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("kernel", choices=["tf32x3", "zgemm", "lu", "step", "linear", "summarize"])
+    ap.add_argument("kernel", choices=["tf32x3", "zgemm", "lu", "step", "linear", "raster",
+                                       "summarize"])
+    ap.add_argument("--slices", type=int, default=8)
     ap.add_argument("csv", nargs="?", help="ncu --csv launch list (summarize)")
     ap.add_argument("--n", type=int, default=961)
     ap.add_argument("--batch", type=int, default=4)
@@ -159,6 +179,9 @@ def main(argv=None) -> int:
         return 0
     if a.kernel == "linear":
         print(json.dumps(_linear(a)))
+        return 0
+    if a.kernel == "raster":
+        print(json.dumps(_raster(a)))
         return 0
     n, b = a.n, a.batch
     s = torch.cuda.current_stream().cuda_stream

@@ -97,6 +97,24 @@ int euv_mask_spectrum(const uint8_t* d_bits, int n_masks, int ndivx, int ndivy, 
                       void* d_work, size_t work_bytes, void* stream);
 
 /* ------------------------------------------------------------------------ */
+/* Mask rasteriser: replaces the pixel fill of the reference's mask generator
+ * (cnn/intensity/mask/mVBF.h:2-70) and its bit packing (mask.cpp:9-26) for
+ * bulk data generation on the device.
+ *
+ * Every mask starts as vacuum (1); d_rects[r] = {mask, x0, x1, y0, y1}
+ * (half-open pixel ranges, clipped to the grid) are painted absorber (0).
+ * Slice s is the drawn mask with the absorber eroded by h_erosion[s] steps of
+ * the 4-neighbour cross (periodic edges; 0 = as drawn) -- a sloped sidewall
+ * (n_slices <= 64).  Output d_bits[mask][slice][ndivx*ndivy/8] in the mask.bin
+ * layout (bit ndivx*y + x, MSB first, 1 = vacuum), ready for
+ * euv_mask_spectrum.  h_erosion is HOST memory.  Workspace:
+ * euv_mask_raster_workspace_bytes (two byte images per mask). */
+size_t euv_mask_raster_workspace_bytes(int n_masks, int ndivx, int ndivy);
+int euv_mask_raster(int n_masks, int ndivx, int ndivy, int n_rects, const int* d_rects,
+                    int n_slices, const int* h_erosion, uint8_t* d_bits, void* d_work,
+                    size_t work_bytes, void* stream);
+
+/* ------------------------------------------------------------------------ */
 /* Batched ampS: replaces ampS (header.h:1208-1466) with multilayerS
  * (header.h:5-363), absorberS0 (754-1145), absorberS (365-752), matinv and
  * matproduct (1468-1619), for n_units independent problems that share one

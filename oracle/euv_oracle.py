@@ -202,6 +202,48 @@ def read_mask_bin(path: str, ndivx: int, ndivy: int, index: int = 0) -> np.ndarr
 
 
 # --------------------------------------------------------------------------
+# Mask generator (cnn/intensity/mask/mVBF.h, mask.cpp)
+# --------------------------------------------------------------------------
+def vbf_mask(ndivx: int, ndivy: int, rand, cd: int = 56, gap: int = 80) -> np.ndarray:
+    """One mask of the reference generator, mask2d[ndivx*j + i] (1 = vacuum),
+    drawing from ``rand`` (a callable returning the C library's rand() values):
+    columns of width cd alternate between all-vacuum stripes and absorber lines
+    broken along y into runs of gap * (rand() % 5) (+ 3 gap for absorber runs)
+    (mVBF.h:2-70, including its tail rules)."""
+    m = np.zeros((ndivy, ndivx), np.int32)          # m[j][i]
+    col = np.zeros(ndivy, np.int32)                  # mask1dY, kept across stripes
+
+    def randmask():                                  # mVBF.h:41-70
+        line = rand() % 2
+        s = 0
+        while s < ndivy - gap:
+            a = gap * (rand() % 5)
+            if line == 1:
+                a += 3 * gap
+            col[s:min(s + a, ndivy)] = 0 if line == 1 else 1
+            line = 0 if line == 1 else 1
+            s += a
+        col[s:] = 0 if line == 0 else 1
+
+    space = rand() % 2                               # mVBF.h:9-29
+    s = 0
+    while s < ndivx - cd:
+        if space == 1:
+            m[:, s:min(s + cd, ndivx)] = 1
+            space = 0
+        else:
+            randmask()
+            m[:, s:min(s + cd, ndivx)] = col[:, None]
+            space = 1
+        s += cd
+    if space == 0:                                   # mVBF.h:30-38
+        m[:, s:] = 0
+    else:
+        m[:, s:] = col[:, None]
+    return m.reshape(-1)
+
+
+# --------------------------------------------------------------------------
 # Order sets, pupil set, sources
 # --------------------------------------------------------------------------
 def order_set(kind: str, LMAX: int, MMAX: int) -> Tuple[np.ndarray, np.ndarray]:
