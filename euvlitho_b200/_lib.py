@@ -22,6 +22,7 @@ EUV_ERR_TIMEOUT = 5
 EUV_STATUS_TIMEOUT = 1
 EUV_STATUS_STEPS_CLAMPED = 2
 EUV_STATUS_SINGULAR = 4
+EUV_STATUS_NOT_CONVERGED = 8
 EUV_MAX_SLICES = 32
 EUV_PREC_FP64 = 0
 EUV_PREC_MIXED = 1
@@ -36,6 +37,7 @@ EXPORTS = (
     "euv_zgemm", "euv_zgemm_tf32x3_workspace_bytes", "euv_zgemm_tf32x3", "euv_lu_workspace_bytes", "euv_lu_factor", "euv_lu_solve",
     "euv_matfun_workspace_bytes", "euv_matfun_cs", "euv_matfun_cs_noalloc",
     "euv_wait_probe", "euv_linear_amp", "euv_mask_raster_workspace_bytes", "euv_mask_raster",
+    "euv_heev_workspace_bytes", "euv_heev", "euv_socs_workspace_bytes", "euv_socs_image",
 )
 
 
@@ -118,6 +120,19 @@ class LinearDesc(C.Structure):
     ]
 
 
+class SocsDesc(C.Structure):
+    _fields_ = [
+        ("n_clips", C.c_int), ("ncut", C.c_int), ("lpx", C.c_int), ("lpy", C.c_int),
+        ("nsocs", C.c_int), ("nsocsxy", C.c_int), ("nout", C.c_int), ("xdiv", C.c_int),
+        ("ydiv", C.c_int), ("d_lp", P), ("d_mp", P),
+        ("k", C.c_double), ("dx", C.c_double), ("dy", C.c_double), ("kx0", C.c_double),
+        ("ky0", C.c_double), ("z0", C.c_double), ("amp_vc", c64), ("amp_ab", c64),
+        ("d_phi_s0", P), ("d_phi_sx", P), ("d_phi_sy", P),
+        ("d_alpha_s0", P), ("d_alpha_sx", P), ("d_alpha_sy", P),
+        ("d_e", P), ("d_kxT", P), ("d_ky", P),
+    ]
+
+
 _lib: Optional[C.CDLL] = None
 
 
@@ -162,6 +177,14 @@ def _declare(lib: C.CDLL) -> None:
     lib.euv_mask_raster_workspace_bytes.restype = sz
     lib.euv_mask_raster_workspace_bytes.argtypes = [i, i, i]
     lib.euv_mask_raster.restype = i
+    lib.euv_heev_workspace_bytes.restype = sz
+    lib.euv_heev_workspace_bytes.argtypes = [i]
+    lib.euv_heev.restype = i
+    lib.euv_socs_workspace_bytes.restype = sz
+    lib.euv_socs_workspace_bytes.argtypes = [C.POINTER(SocsDesc)]
+    lib.euv_socs_image.restype = i
+    lib.euv_socs_image.argtypes = [C.POINTER(SocsDesc), P, P, P, P, P, P, sz, P]
+    lib.euv_heev.argtypes = [i, P, i, P, P, i, i, d, P, sz, P, P]
     lib.euv_mask_raster.argtypes = [i, i, i, i, P, i, P, P, P, sz, P]
     lib.euv_linear_amp.argtypes = [C.POINTER(LinearDesc), P, P, P, P, P, P]
     lib.euv_wait_probe.argtypes = [P, ll, P, P]
@@ -194,6 +217,7 @@ _STATUS_TEXT = (
     (EUV_STATUS_TIMEOUT, "a bounded device wait gave up (results incomplete)"),
     (EUV_STATUS_STEPS_CLAMPED, "a unit needed more double-angle steps than m_max"),
     (EUV_STATUS_SINGULAR, "an LU met an exactly zero pivot"),
+    (EUV_STATUS_NOT_CONVERGED, "an eigensolver stopped at its sweep limit"),
 )
 
 

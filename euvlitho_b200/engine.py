@@ -467,6 +467,89 @@ class Plan:
         return out[0], (out[1] if thin else None)
 
 
+    # ------------------------------------------------------------ STCC-SOCS
+    def socs_tables(self, z: Optional[float] = None, nsocs: int = 100, nsocsxy: int = 20,
+                    nout: int = 64, mesh_deg: float = 0.2, max_sweeps: int = 30):
+        """Resident SOCS kernels (eigenfunction.py:5-163): the three TCC
+        matrices over the linear model's source grid as device GEMMs, their
+        eigenpairs by the device Jacobi solver (euv_heev), the nsocs / nsocsxy
+        kernels of largest |alpha|, and the DFT / interpolation tables."""
+        cfg = self.cfg
+        z = float(cfg.z if z is None else z)
+        key = (z, nsocs, nsocsxy, nout, mesh_deg)
+        tb = getattr(self, "_socs_tables", None)
+        if tb is not None and tb["key"] == key:
+            return tb
+        n = self.ncut
+        if nsocs > n or nsocsxy > nsocs:
+            raise ValueError("need nsocsxy <= nsocs <= %d pupil points" % n)
+        dsx, dsy = T.linear_sources(cfg, mesh_deg)
+        S = len(dsx)
+        P, w0 = T.socs_phase(cfg, z, dsx, dsy, self.linput, self.minput)
+        pall = np.concatenate([P[0], P[1], P[2]], axis=1)                 # [n, 3S]
+        dev = self.device
+        a_cm = torch.from_numpy(np.ascontiguousarray(pall.T)).to(dev)      # column-major n x 3S
+        lib = L.lib()
+        wb = lib.euv_heev_workspace_bytes(n)
+        hw = torch.empty(wb, dtype=torch.uint8, device=dev)
+        out = {}
+        for name, wt in (("s0", np.ones(S)), ("sx", dsx), ("sy", dsy)):
+            q = torch.from_numpy(np.conj(pall) * np.tile(wt * w0, 3)[None, :]).to(dev)  # col-major 3S x n
+            tcc = torch.empty((n, n), dtype=torch.complex128, device=dev)
+            L.call("euv_zgemm", n, n, 3 * S, L.c64.of(1.0 / S), None, a_cm.data_ptr(), n, 0,
+                   q.data_ptr(), 3 * S, 0, L.c64.of(0), tcc.data_ptr(), n, 0, L.c64.of(0), 1,
+                   None, 0, _stream())
+            del q
+            w = torch.empty(n, dtype=torch.float64, device=dev)
+            v = torch.empty((n, n), dtype=torch.complex128, device=dev)
+            L.call("euv_heev", n, tcc.data_ptr(), n, w.data_ptr(), v.data_ptr(), n, max_sweeps,
+                   1e-14, hw.data_ptr(), wb, self.status.data_ptr(), _stream())
+            self.check()
+            wh = w.cpu().numpy()
+            order = np.lexsort((wh, -np.abs(wh)))   # |alpha| descending, ties ascending
+            keep = nsocs if name == "s0" else nsocsxy
+            idx = torch.from_numpy(order[:max(keep, 1)].astype(np.int64)).to(dev)
+            out["alpha_" + name] = self._f64(wh[order[:max(keep, 1)]])
+            out["phi_" + name] = v.index_select(0, idx).contiguous()  # row m = eigenvector m
+            out["eig_" + name] = wh[order]
+        E, Kx, Ky = T.socs_interp_tables(nout, cfg.xdiv, cfg.ydiv)
+        u = self.uniform_solves()
+        tb = dict(key=key, nsocs=nsocs, nsocsxy=nsocsxy, nout=nout, n_src=S,
+                  e=self._c128(E), kxT=self._c128(Kx), ky=self._c128(np.ascontiguousarray(Ky.T)),
+                  lp=self._i32(self.linput), mp=self._i32(self.minput),
+                  amp_vc=complex(u["ax_vc"][u["s_center"], u["n00"]].item()),
+                  amp_ab=complex(u["ax_ab"][u["s_center"], u["n00"]].item()), **out)
+        self._socs_tables = tb
+        return tb
+
+    def socs(self, masks, a0, ax, ay, z: Optional[float] = None, **kw) -> torch.Tensor:
+        """STCC-SOCS images [clips, XDIV, YDIV] from the M3D parameters
+        (socs.py:12-151; a0, ax, ay as for ``linear``)."""
+        cfg = self.cfg
+        tb = self.socs_tables(z, **kw)
+        m = self.as_mask_tensor(masks)
+        nc, ncut = m.shape[0], self.ncut
+        par = [torch.as_tensor(v).to(self.device, torch.complex128).reshape(nc, ncut).contiguous()
+               for v in (a0, ax, ay)]
+        fvac = self.spectra(m[:, :1], cfg.lpmaxX, cfg.lpmaxY, select_vacuum=1, per_slice=False)
+        d = L.SocsDesc()
+        d.n_clips, d.ncut, d.lpx, d.lpy = nc, ncut, cfg.lpmaxX, cfg.lpmaxY
+        d.nsocs, d.nsocsxy, d.nout, d.xdiv, d.ydiv = tb["nsocs"], tb["nsocsxy"], tb["nout"], cfg.xdiv, cfg.ydiv
+        d.d_lp, d.d_mp = _ptr(tb["lp"]), _ptr(tb["mp"])
+        d.k, d.dx, d.dy, d.kx0, d.ky0, d.z0 = cfg.k, cfg.dx, cfg.dy, cfg.kx0, cfg.ky0, cfg.z0
+        d.amp_vc, d.amp_ab = L.c64.of(tb["amp_vc"]), L.c64.of(tb["amp_ab"])
+        d.d_phi_s0, d.d_phi_sx, d.d_phi_sy = _ptr(tb["phi_s0"]), _ptr(tb["phi_sx"]), _ptr(tb["phi_sy"])
+        d.d_alpha_s0, d.d_alpha_sx, d.d_alpha_sy = (_ptr(tb["alpha_s0"]), _ptr(tb["alpha_sx"]),
+                                                    _ptr(tb["alpha_sy"]))
+        d.d_e, d.d_kxT, d.d_ky = _ptr(tb["e"]), _ptr(tb["kxT"]), _ptr(tb["ky"])
+        wb = L.lib().euv_socs_workspace_bytes(C.byref(d))
+        ws = self.work.get(wb)
+        img = torch.empty((nc, cfg.xdiv, cfg.ydiv), dtype=torch.complex128, device=self.device)
+        L.call("euv_socs_image", C.byref(d), fvac.data_ptr(), par[0].data_ptr(), par[1].data_ptr(),
+               par[2].data_ptr(), img.data_ptr(), ws.data_ptr(), ws.numel(), _stream())
+        return img.real
+
+
 def _check_word(word: torch.Tensor, where: str) -> None:
     bits = int(word.item())
     if bits:

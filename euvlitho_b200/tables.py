@@ -263,3 +263,40 @@ def linear_abbe_table(cfg: SimConfig, dsx, dsy, linput, minput):
     coef = np.where(ok[..., None], (f * phase)[..., None] * R, 0.0).astype(np.complex128)
     nidx = np.where(ok, np.arange(len(linput), dtype=np.int32)[None, :], -1).astype(np.int32)
     return coef, nidx
+
+
+# ----------------------------------------------------------- STCC-SOCS
+def socs_phase(cfg: SimConfig, z: float, dsx, dsy, linput, minput):
+    """Pupil-source phase matrices of the TCC (eigenfunction.py:84-111):
+    P[c][i][s] = phase(i, s) R(c, 0) for pupil point i and source s (zero
+    outside the pupil NA), and the source weight w0[s] = k^2 / (k^2 - (kx0 +
+    dsx_s)^2).  TCC_w = sum_c P_c diag(w w0) P_c^H / S for w = 1, dsx, dsy."""
+    k, dx, dy, MX, MY, NA = cfg.k, cfg.dx, cfg.dy, cfg.mx, cfg.my, cfg.na
+    kx0, ky0, z0 = cfg.kx0, cfg.ky0, cfg.z0
+    dsx = np.asarray(dsx, np.float64)
+    dsy = np.asarray(dsy, np.float64)
+    ksx = (2 * PI / dx * np.asarray(linput, np.float64))[:, None] + dsx[None, :]
+    ksy = (2 * PI / dy * np.asarray(minput, np.float64))[:, None] + dsy[None, :]
+    p2 = MX * MX * ksx * ksx + MY * MY * ksy * ksy
+    phase = np.exp(1j * ((ksx + kx0) ** 2 + (ksy + ky0) ** 2) / 2.0 / k * z0
+                   + 1j * p2 / 2.0 / k * z) * (p2 <= (k * NA) ** 2)
+    R = rotate(k, MX, MY, ksx, ksy, kx0, ky0)[..., 0]  # [n, S, 3]
+    P = np.moveaxis(phase[..., None] * R, -1, 0)       # [3, n, S]
+    w0 = k * k / (k * k - (kx0 + dsx) ** 2)
+    return np.nan_to_num(P), w0
+
+
+def socs_interp_tables(nout: int, xdiv: int, ydiv: int):
+    """DFT matrix E[a][b] = e^{2 pi i a b / nout} and the Fourier-interpolation
+    kernels K[x][u] = (1/nout) sum_{i=-nout/2}^{nout/2-1} e^{2 pi i i (x/xdiv - u/nout)}
+    (socs.py:137-150) for x and y."""
+    a = np.arange(nout)
+    E = np.exp(2j * PI * np.outer(a, a) / nout)
+    i = np.arange(-(nout // 2), nout // 2)
+
+    def kern(xd):
+        x = np.arange(xd)
+        ph = x[:, None, None] / xd - a[None, :, None] / nout  # [x, u, 1]
+        return np.exp(2j * PI * i[None, None, :] * ph).sum(-1) / nout
+
+    return E, kern(xdiv), kern(ydiv)

@@ -48,6 +48,7 @@ extern "C" {
 #define EUV_STATUS_TIMEOUT 1       /* a bounded device wait gave up: that call's results are incomplete */
 #define EUV_STATUS_STEPS_CLAMPED 2 /* a unit needed more double-angle steps than m_max */
 #define EUV_STATUS_SINGULAR 4      /* an LU met an exactly zero pivot */
+#define EUV_STATUS_NOT_CONVERGED 8 /* an eigensolver stopped at its sweep limit */
 
 #define EUV_MAX_SLICES 32
 
@@ -95,6 +96,58 @@ size_t euv_mask_spectrum_workspace_bytes(int n_masks, int ndivx, int ndivy, int 
 int euv_mask_spectrum(const uint8_t* d_bits, int n_masks, int ndivx, int ndivy, int fdivx,
                       int fdivy, int lh, int mh, int select_vacuum, int y_offset, euv_c64* d_out,
                       void* d_work, size_t work_bytes, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Hermitian eigendecomposition (parallel cyclic Jacobi): replaces the eigh of
+ * the STCC-SOCS transmission cross-coefficient matrices
+ * (cnn/intensity/stccsocs/eigenfunction.py:128-130; cupy.linalg.eigh there).
+ * d_a (n x n, column-major, Hermitian) is overwritten (diagonalised);
+ * d_w[i] = eigenvalue i, d_v(:, i) its eigenvector, in no particular order.
+ * Stops when the off-diagonal Frobenius norm is <= tol x the full one, or
+ * after max_sweeps sweeps (EUV_STATUS_NOT_CONVERGED into *d_status then).
+ * A per-configuration step: n - 1 rounds of three launches per sweep. */
+size_t euv_heev_workspace_bytes(int n);
+int euv_heev(int n, euv_c64* d_a, int lda, double* d_w, euv_c64* d_v, int ldv, int max_sweeps,
+             double tol, void* d_work, size_t work_bytes, int* d_status, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* STCC-SOCS image from M3D parameters: replaces intsocs
+ * (cnn/intensity/stccsocs/socs.py:12-151).  For clip c with vacuum-indicator
+ * spectrum F_c (euv_mask_spectrum, select_vacuum = 1, lh = lpx, mh = lpy) and
+ * M3D parameters a0, ax, ay [c][ncut] (ax = ay = 0 without a slope):
+ *   A0 = famp + a0 (famp as in euv_linear_amp), Ax = ax dx/2pi, Ay = ay dy/2pi,
+ *   Axy = ax lp/2 + ay mp/2;
+ *   small = sum_{m<nsocs} alpha_s0[m] |F[A0 phi_s0[m]]|^2
+ *         + sum_{m<nsocsxy} 2 Re(alpha_sx[m] F[A0 phi_sx[m]] F*[Ax phi_sx[m]]
+ *                               + alpha_sy[m] F[A0 phi_sy[m]] F*[Ay phi_sy[m]]
+ *                               + alpha_s0[m] F[A0 phi_s0[m]] F*[Axy phi_s0[m]]),
+ * F[v](x, y) = sum_n v_n e^{2 pi i (lp_n x + mp_n y)/nout} on the nout x nout grid;
+ * d_image[c][x][y] = sum_{u,v} Kx[x][u] small[u][v] Ky[y][v] (complex; its real
+ * part is the image), Kx[x][u] = (1/nout) sum_{i=-nout/2}^{nout/2-1}
+ * e^{2 pi i i (x/xdiv - u/nout)} (Ky alike): the Fourier interpolation of
+ * socs.py:137-150.  phi_*[m][n]: eigenfunction m of the TCC at pupil point n
+ * (euv_heev + sort by |alpha|).  The resident tables d_e, d_kxT, d_ky are
+ * config-only. */
+typedef struct {
+  int n_clips, ncut, lpx, lpy, nsocs, nsocsxy, nout, xdiv, ydiv;
+  const int* d_lp;             /* [ncut] pupil orders */
+  const int* d_mp;
+  double k, dx, dy, kx0, ky0, z0;
+  euv_c64 amp_vc, amp_ab;      /* specular amplitudes of the all-vacuum / all-absorber mask */
+  const euv_c64* d_phi_s0;     /* [nsocs][ncut] */
+  const euv_c64* d_phi_sx;     /* [nsocsxy][ncut] */
+  const euv_c64* d_phi_sy;
+  const double* d_alpha_s0;    /* [nsocs] */
+  const double* d_alpha_sx;    /* [nsocsxy] */
+  const double* d_alpha_sy;
+  const euv_c64* d_e;          /* [nout][nout] e^{2 pi i a b / nout} */
+  const euv_c64* d_kxT;        /* element u + nout x = Kx[x][u] */
+  const euv_c64* d_ky;         /* element y + ydiv v = Ky[y][v] */
+} euv_socs_desc;
+size_t euv_socs_workspace_bytes(const euv_socs_desc* desc);
+int euv_socs_image(const euv_socs_desc* desc, const euv_c64* d_fvac, const euv_c64* d_a0,
+                   const euv_c64* d_ax, const euv_c64* d_ay, euv_c64* d_image, void* d_work,
+                   size_t work_bytes, void* stream);
 
 /* ------------------------------------------------------------------------ */
 /* Mask rasteriser: replaces the pixel fill of the reference's mask generator

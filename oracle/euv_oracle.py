@@ -986,6 +986,90 @@ def linear_image(cfg: SimConfig, amp, dsx, dsy, linput, minput, z: float = 0.0,
     return isum
 
 
+# --------------------------------------------------------------------------
+# STCC-SOCS imaging (cnn/intensity/stccsocs/eigenfunction.py, socs.py)
+# --------------------------------------------------------------------------
+def socs_tcc(cfg: SimConfig, z: float = 0.0, mesh_deg: float = 0.2):
+    """The three transmission cross-coefficient matrices (eigenfunction.py:5-124)
+    on the pupil points: TCC_w = sum_c P_c diag(w k^2/(k^2 - (kx0+dsx)^2)) P_c^H / S
+    for w = 1, dsx, dsy, with P_c[i, s] = phase(i, s) R(c, 0) (zero outside the
+    pupil NA) over the linear model's source grid.  Returns (s0, sx, sy)."""
+    k, dx, dy, MX, MY, NA = cfg.k, cfg.dx, cfg.dy, cfg.mx, cfg.my, cfg.na
+    kx0, ky0, z0 = cfg.kx0, cfg.ky0, cfg.z0
+    dsx, dsy = linear_sources(cfg, mesh_deg)
+    lin, mn, _, _ = pupil_set(cfg)
+    S, n = len(dsx), len(lin)
+    ksx = (2 * PI / dx * lin)[:, None] + dsx[None, :]
+    ksy = (2 * PI / dy * mn)[:, None] + dsy[None, :]
+    p2 = MX * MX * ksx * ksx + MY * MY * ksy * ksy
+    phase = np.exp(1j * ((ksx + kx0) ** 2 + (ksy + ky0) ** 2) / 2.0 / k * z0
+                   + 1j * p2 / 2.0 / k * z) * (p2 <= (k * NA) ** 2)
+    R = rotate_many(k, MX, MY, ksx.ravel(), ksy.ravel(), kx0, ky0)[:, :, 0].reshape(n, S, 3)
+    w0 = k * k / (k * k - (kx0 + dsx) ** 2)
+    out = []
+    for wt in (w0, dsx * w0, dsy * w0):
+        t = np.zeros((n, n), np.complex128)
+        for c in range(3):
+            P = phase * R[:, :, c]
+            t += P @ (np.conj(P).T * wt[:, None])
+        out.append(t / S)
+    return tuple(out)
+
+
+def socs_eigen(tcc):
+    """Eigenpairs of one TCC sorted by |alpha|, largest first, ties in
+    ascending-eigenvalue order (eigenfunction.py:125-163).  Returns (alpha,
+    phi) with phi[m] the m-th eigenvector."""
+    w, v = np.linalg.eigh(tcc)
+    order = np.argsort(-np.abs(w), kind="stable")
+    return w[order], v[:, order].T.copy()
+
+
+def socs_image(cfg: SimConfig, mask2d, a0, ax, ay, ampvc, ampab, eig, nsocs: int = 100,
+               nsocsxy: int = 20, nout: int = 64) -> np.ndarray:
+    """SOCS image from the M3D parameters (socs.py:12-151): the kernels of the
+    three TCCs weighted by the pupil amplitudes on an nout x nout grid, the
+    |.|^2 sum (plus the first-order cross terms of ax, ay), and Fourier
+    interpolation to XDIV x YDIV.  a0, ax, ay: one value per pupil point.
+    ``eig`` = (alpha_s0, phi_s0, alpha_sx, phi_sx, alpha_sy, phi_sy).
+    Returns the real part (what socs.py writes)."""
+    a_s0, p_s0, a_sx, p_sx, a_sy, p_sy = eig
+    dx, dy = cfg.dx, cfg.dy
+    lin, mn, _, _ = pupil_set(cfg)
+    famp = linear_amplitudes(cfg, mask2d, np.zeros(len(lin)), np.zeros(len(lin)),
+                             np.zeros(len(lin)), ampvc, ampab, [0.0], [0.0], lin, mn)[1][0]
+    a0, ax, ay = np.asarray(a0), np.asarray(ax), np.asarray(ay)
+    A0 = famp + a0
+    Ax = ax * dx / (2 * PI)
+    Ay = ay * dy / (2 * PI)
+    Axy = ax * lin / 2.0 + ay * mn / 2.0
+    px, py = lin % nout, mn % nout
+
+    def field(v):
+        g = np.zeros((nout, nout), np.complex128)
+        g[px, py] = v
+        return np.fft.ifft2(g) * nout * nout
+
+    small = np.zeros((nout, nout))
+    for m in range(nsocs):
+        f0 = field(A0 * p_s0[m])
+        small += a_s0[m] * np.abs(f0) ** 2
+        if m < nsocsxy:
+            f0x, fx = field(A0 * p_sx[m]), field(Ax * p_sx[m])
+            f0y, fy = field(A0 * p_sy[m]), field(Ay * p_sy[m])
+            fxy = field(Axy * p_s0[m])
+            small += 2 * a_sx[m] * (f0x * np.conj(fx)).real + 2 * a_sy[m] * (f0y * np.conj(fy)).real \
+                + 2 * a_s0[m] * (f0 * np.conj(fxy)).real
+    spec = np.fft.fft2(small) / nout / nout
+    XD, YD = cfg.xdiv, cfg.ydiv
+    big = np.zeros((XD, YD), np.complex128)
+    h = nout // 2
+    for i in range(-h, h):
+        for j in range(-h, h):
+            big[i, j] = spec[i, j]
+    return (np.fft.ifft2(big) * XD * YD).real
+
+
 def expand_xinput(values, xinput):
     """Slopes stored for the xinput points only (inputxx.csv rows 3-6) -> one
     value per pupil point, zero elsewhere."""

@@ -73,7 +73,7 @@ def test_descriptor_layout_matches_the_header(tmp_path):
     ctypes mirrors."""
     import subprocess
     structs = {"euv_amp_desc": L.AmpDesc, "euv_abbe_desc": L.AbbeDesc, "euv_m3d_desc": L.M3dDesc,
-               "euv_stack": L.Stack, "euv_linear_desc": L.LinearDesc}
+               "euv_stack": L.Stack, "euv_linear_desc": L.LinearDesc, "euv_socs_desc": L.SocsDesc}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "euvl_b200.h"', "int main(void) {"]
     for cname, py in structs.items():
         lines.append('printf("%s size %%zu\\n", sizeof(%s));' % (cname, cname))
