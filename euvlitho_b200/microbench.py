@@ -6,6 +6,7 @@
   python -m euvlitho_b200.microbench step   --precision mixed --clips 4
   python -m euvlitho_b200.microbench linear --preset reference --clips 1
   python -m euvlitho_b200.microbench raster --clips 64 --slices 8
+  python -m euvlitho_b200.microbench socs   --preset reference --clips 4
   python -m euvlitho_b200.microbench summarize launches.csv
 
 Times each library entry point with CUDA events on the launching stream after
@@ -20,6 +21,8 @@ form's intensity error against it.
 Abbe images per clip) with tables resident, on seeded masks and parameters.
 `raster` times the device mask rasteriser on the reference generator's
 2048^2 masks (layouts drawn on the host beforehand), with sidewall slices.
+`socs` times the STCC-SOCS tables (TCC GEMMs + three Jacobi eigensolves, once
+per configuration) and the per-clip SOCS images.
 `summarize` folds an ncu `--csv` launch list of gpu__time_duration.sum into
 launches, total time and share per kernel.
 """
@@ -140,6 +143,30 @@ def _raster(a) -> dict:
             "masks_per_s": n / (ms / 1e3), "gb_per_s_algorithmic": moved / (ms / 1e3) / 1e9}
 
 
+def _socs(a) -> dict:
+    import time
+    import numpy as np
+    from . import masks as MK
+    from .config import preset
+    from .engine import Plan
+    cfg = preset(a.preset)
+    plan = Plan(cfg, device=torch.device("cuda"))
+    plan.uniform_solves()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    tb = plan.socs_tables()
+    torch.cuda.synchronize()
+    t_tab = time.perf_counter() - t0
+    rng = np.random.default_rng(0)
+    par = [torch.from_numpy((rng.standard_normal((a.clips, plan.ncut))
+                             + 1j * rng.standard_normal((a.clips, plan.ncut))) * 1e-3).cuda()
+           for _ in range(3)]
+    bits = torch.from_numpy(MK.batch(cfg.ndivx, cfg.ndivy, range(a.clips))).cuda()
+    ms = _time(lambda: plan.socs(bits, *par), a.reps)
+    return {"preset": a.preset, "clips": a.clips, "ncut": plan.ncut, "sources": tb["n_src"],
+            "tables_s": t_tab, "ms_per_call": ms, "clips_per_s": a.clips / (ms / 1e3)}
+
+
 def _time(fn, reps: int) -> float:
     for _ in range(3):
         fn()
@@ -158,7 +185,7 @@ def _time(fn, reps: int) -> float:
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("kernel", choices=["tf32x3", "zgemm", "lu", "step", "linear", "raster",
-                                       "summarize"])
+                                       "socs", "summarize"])
     ap.add_argument("--slices", type=int, default=8)
     ap.add_argument("csv", nargs="?", help="ncu --csv launch list (summarize)")
     ap.add_argument("--n", type=int, default=961)
@@ -182,6 +209,9 @@ def main(argv=None) -> int:
         return 0
     if a.kernel == "raster":
         print(json.dumps(_raster(a)))
+        return 0
+    if a.kernel == "socs":
+        print(json.dumps(_socs(a)))
         return 0
     n, b = a.n, a.batch
     s = torch.cuda.current_stream().cuda_stream
