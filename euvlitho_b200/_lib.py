@@ -94,7 +94,7 @@ class AbbeDesc(C.Structure):
         ("ncut", C.c_int), ("n_units", C.c_int), ("n_src", C.c_int), ("n_order", C.c_int),
         ("d_coef", P), ("d_nidx", P), ("d_px", P), ("d_py", P), ("d_row_start", P),
         ("d_tab_of_unit", P), ("d_img_of_unit", P), ("d_nsrc_of_unit", P),
-        ("n_images", C.c_int), ("d_inv_weight", P),
+        ("n_images", C.c_int), ("d_inv_weight", P), ("precision", C.c_int),
     ]
 
 

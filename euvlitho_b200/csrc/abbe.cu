@@ -18,6 +18,29 @@
 
 namespace euv {
 
+// complex arithmetic in the kernel's type R (double: FP64 form; float: the
+// mixed form, whose DFT sums need ~1e-6, not 1e-16)
+template <typename R>
+struct cx {
+  R x, y;
+};
+template <typename R>
+__device__ __forceinline__ cx<R> operator+(cx<R> a, cx<R> b) { return {a.x + b.x, a.y + b.y}; }
+template <typename R>
+__device__ __forceinline__ cx<R> operator*(cx<R> a, cx<R> b) {
+  return {a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
+}
+template <typename R>
+struct vec2;
+template <>
+struct vec2<double> {
+  using type = double2;
+};
+template <>
+struct vec2<float> {
+  using type = float2;
+};
+
 constexpr int AB_YS = 4;
 constexpr int AB_THREADS = 256;
 constexpr int AB_XPT = 4;  // x values per thread: xdiv <= 1024
@@ -34,12 +57,15 @@ struct AbbeParams {
   const double* inv_weight;
 };
 
+template <typename R>
 __global__ void __launch_bounds__(AB_THREADS) abbe_kernel(AbbeParams p, const double2* ax,
                                                           double* image) {
-  extern __shared__ double2 sm[];
-  double2* E = sm;                                   // [ncut][3]
-  double2* G = E + (size_t)p.ncut * 3;                // [YS][bx][3]
-  double2* twy = G + (size_t)AB_YS * p.bx * 3;        // [YS][by]
+  using V2 = typename vec2<R>::type;
+  using C = cx<R>;
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  V2* E = reinterpret_cast<V2*>(sm_raw);              // [ncut][3]
+  V2* G = E + (size_t)p.ncut * 3;                     // [YS][bx][3]
+  V2* twy = G + (size_t)AB_YS * p.bx * 3;             // [YS][by]
   const int u = blockIdx.z;
   const int y0 = blockIdx.x * AB_YS;
   const int tid = threadIdx.x;
@@ -53,7 +79,7 @@ __global__ void __launch_bounds__(AB_THREADS) abbe_kernel(AbbeParams p, const do
     if (q < 0) q += p.ydiv;
     double s, c;
     sincospi(2.0 * (double)q / (double)p.ydiv, &s, &c);
-    twy[idx] = make_double2(c, s);
+    twy[idx] = V2{(R)c, (R)s};
   }
 
   double acc[AB_XPT][AB_YS];
@@ -77,22 +103,22 @@ __global__ void __launch_bounds__(AB_THREADS) abbe_kernel(AbbeParams p, const do
         e1 = mk(cf[1].x, cf[1].y) * a;
         e2 = mk(cf[2].x, cf[2].y) * a;
       }
-      E[i * 3 + 0] = make_double2(e0.x, e0.y);
-      E[i * 3 + 1] = make_double2(e1.x, e1.y);
-      E[i * 3 + 2] = make_double2(e2.x, e2.y);
+      E[i * 3 + 0] = V2{(R)e0.x, (R)e0.y};
+      E[i * 3 + 1] = V2{(R)e1.x, (R)e1.y};
+      E[i * 3 + 2] = V2{(R)e2.x, (R)e2.y};
     }
     __syncthreads();
     // stage y
     for (int o = tid; o < AB_YS * p.bx * 3; o += AB_THREADS) {
       const int c = o % 3, lx = (o / 3) % p.bx, yy = o / (3 * p.bx);
-      cplx g = mk(0, 0);
+      C g{(R)0, (R)0};
       const int i0 = p.row_start[lx], i1 = p.row_start[lx + 1];
       for (int i = i0; i < i1; ++i) {
-        double2 e = E[i * 3 + c];
-        double2 t = twy[yy * p.by + (p.py[i] + p.lpy)];
-        g = g + mk(e.x, e.y) * mk(t.x, t.y);
+        const V2 e = E[i * 3 + c];
+        const V2 t = twy[yy * p.by + (p.py[i] + p.lpy)];
+        g = g + C{e.x, e.y} * C{t.x, t.y};
       }
-      G[o] = make_double2(g.x, g.y);
+      G[o] = V2{g.x, g.y};
     }
     __syncthreads();
     // stage x + |f|^2
@@ -105,26 +131,26 @@ __global__ void __launch_bounds__(AB_THREADS) abbe_kernel(AbbeParams p, const do
         double s0, c0, s1, c1;
         sincospi(2.0 * (double)q0 / (double)p.xdiv, &s0, &c0);
         sincospi(2.0 * (double)x / (double)p.xdiv, &s1, &c1);
-        cplx w = mk(c0, s0);
-        const cplx r = mk(c1, s1);
-        cplx f[AB_YS][3];
+        C w{(R)c0, (R)s0};
+        const C r{(R)c1, (R)s1};
+        C f[AB_YS][3];
 #pragma unroll
-        for (int b = 0; b < AB_YS; ++b) f[b][0] = f[b][1] = f[b][2] = mk(0, 0);
+        for (int b = 0; b < AB_YS; ++b) f[b][0] = f[b][1] = f[b][2] = C{(R)0, (R)0};
         for (int lx = 0; lx < p.bx; ++lx) {
 #pragma unroll
           for (int b = 0; b < AB_YS; ++b) {
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-              double2 g = G[(b * p.bx + lx) * 3 + c];
-              f[b][c] = f[b][c] + mk(g.x, g.y) * w;
+              const V2 g = G[(b * p.bx + lx) * 3 + c];
+              f[b][c] = f[b][c] + C{g.x, g.y} * w;
             }
           }
           w = w * r;
         }
 #pragma unroll
         for (int b = 0; b < AB_YS; ++b)
-          acc[a][b] += f[b][0].x * f[b][0].x + f[b][0].y * f[b][0].y + f[b][1].x * f[b][1].x +
-                       f[b][1].y * f[b][1].y + f[b][2].x * f[b][2].x + f[b][2].y * f[b][2].y;
+          acc[a][b] += (double)(f[b][0].x * f[b][0].x + f[b][0].y * f[b][0].y + f[b][1].x * f[b][1].x +
+                                f[b][1].y * f[b][1].y + f[b][2].x * f[b][2].x + f[b][2].y * f[b][2].y);
       }
     }
   }
@@ -150,7 +176,8 @@ extern "C" int euv_abbe(const euv_abbe_desc* d, const euv_c64* d_ax, double* d_i
       d->xdiv > AB_THREADS * AB_XPT || d->lpx < 0 || d->lpy < 0 || d->ncut <= 0 ||
       d->n_units <= 0 || d->n_src <= 0 || d->n_order <= 0 || !d->d_coef || !d->d_nidx ||
       !d->d_px || !d->d_py || !d->d_row_start || !d->d_tab_of_unit || !d->d_img_of_unit || !d->d_nsrc_of_unit || !d->d_inv_weight ||
-      d->n_images <= 0 || d->n_units > 65535) {
+      d->n_images <= 0 || d->n_units > 65535 ||
+      (d->precision != EUV_PREC_FP64 && d->precision != EUV_PREC_MIXED)) {
     euv_set_error("euv_abbe: bad arguments");
     return EUV_ERR_BAD_ARG;
   }
@@ -178,17 +205,25 @@ extern "C" int euv_abbe(const euv_abbe_desc* d, const euv_c64* d_ax, double* d_i
   if (nsplit < 1) nsplit = 1;
   if (nsplit > d->n_src) nsplit = d->n_src;
   p.nsplit = nsplit;
+  const bool fp32 = d->precision == EUV_PREC_MIXED;
   size_t smem = ((size_t)d->ncut * 3 + (size_t)AB_YS * p.bx * 3 + (size_t)AB_YS * p.by) *
-                sizeof(double2);
+                (fp32 ? sizeof(float2) : sizeof(double2));
   if (smem > 227 * 1024) {
     euv_set_error("euv_abbe: pupil too large for one CTA (%zu bytes of shared memory)", smem);
     return EUV_ERR_BAD_ARG;
   }
-  static int smem_done[64];
-  EUV_CUDA_TRY(ensure_smem(abbe_kernel, (int)smem, smem_done));
   dim3 grid(ystripes, nsplit, d->n_units);
-  abbe_kernel<<<grid, AB_THREADS, smem, stream>>>(p, reinterpret_cast<const double2*>(d_ax),
-                                                  d_image);
+  if (fp32) {
+    static int smem_done[64];
+    EUV_CUDA_TRY(ensure_smem(abbe_kernel<float>, (int)smem, smem_done));
+    abbe_kernel<float><<<grid, AB_THREADS, smem, stream>>>(p, reinterpret_cast<const double2*>(d_ax),
+                                                           d_image);
+  } else {
+    static int smem_done[64];
+    EUV_CUDA_TRY(ensure_smem(abbe_kernel<double>, (int)smem, smem_done));
+    abbe_kernel<double><<<grid, AB_THREADS, smem, stream>>>(p, reinterpret_cast<const double2*>(d_ax),
+                                                            d_image);
+  }
   EUV_LAUNCH_CHECK();
   return EUV_OK;
 }

@@ -614,6 +614,7 @@ class IntensityBatch:
         ad.d_nsrc_of_unit = _ptr(self.t_ns)
         ad.n_images = nc * npol
         ad.d_inv_weight = _ptr(self.inv_w)
+        ad.precision = plan.precision  # mixed: the Abbe DFT sums in FP32
         self.adesc = ad
         lib = L.lib()
         self.spec_bytes = lib.euv_mask_spectrum_workspace_bytes(nc * n_mask_slices, cfg.ndivx, cfg.ndivy,

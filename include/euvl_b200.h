@@ -271,6 +271,7 @@ typedef struct {
   const int* d_nsrc_of_unit;  /* [U] */
   int n_images;
   const double* d_inv_weight; /* [n_images] 1/SDIVSUM */
+  int precision;               /* EUV_PREC_FP64, or EUV_PREC_MIXED: DFT sums in FP32 */
 } euv_abbe_desc;
 
 int euv_abbe(const euv_abbe_desc* desc, const euv_c64* d_ax, double* d_image, void* stream);
