@@ -122,8 +122,10 @@ __global__ void __launch_bounds__(LU_PANEL_THREADS) lu_panel_kernel(int n, int j
 // r0 + t + k*LP_THREADS (k < RPT) of the sub-panel in registers, so pivot
 // search, row exchange, scaling and the rank-1 updates inside the sub-panel
 // touch no global memory.  After each sub-panel, the rest of the panel is
-// brought up to date at once (U12 = L11^-1 A12, A22 -= L21 U12): one global
-// read-modify-write per sub-panel instead of one per column.
+// brought up to date at once: its row swaps and U12 = L11^-1 A12 by one thread
+// per column (rows gathered into registers, L11 from shared memory), then
+// A22 -= L21 U12 with batched loads.  The panel's columns left of a sub-panel
+// get its swaps from the laswp launch that follows the panel (sub = LP_SB).
 constexpr int LP_THREADS = 512;
 constexpr int LP_SB = 4;
 
@@ -139,6 +141,8 @@ __global__ void __launch_bounds__(LP_THREADS) lu_panel_reg_kernel(int n, int j0,
   __shared__ int s_piv;
   __shared__ cplx s_rowa[LP_SB], s_rowb[LP_SB], s_prow[LP_SB];
   __shared__ cplx s_u12[LP_SB][LU_NB];
+  __shared__ cplx s_l11[LP_SB][LP_SB];
+  __shared__ int s_pivs[LP_SB];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (int sub = 0; sub < jb; sub += LP_SB) {
     const int sb = (jb - sub) < LP_SB ? (jb - sub) : LP_SB;
@@ -191,6 +195,7 @@ __global__ void __launch_bounds__(LP_THREADS) lu_panel_reg_kernel(int n, int j0,
           }
         if (bi >= n) bi = jj;
         s_piv = bi;
+        s_pivs[c] = bi;
         ipiv[jj] = bi;
       }
       __syncthreads();
@@ -204,13 +209,6 @@ __global__ void __launch_bounds__(LP_THREADS) lu_panel_reg_kernel(int n, int j0,
             if (r == jj) s_rowa[cc] = v[k][cc];
             if (r == piv) s_rowb[cc] = v[k][cc];
           }
-        }
-        // the panel's other columns: exchange rows jj and piv in global memory
-        for (int t = tid; t < jb - sb; t += LP_THREADS) {
-          const int col = t < sub ? j0 + t : j0 + t + sb;
-          double2 x = A[jj + (long long)col * lda];
-          A[jj + (long long)col * lda] = A[piv + (long long)col * lda];
-          A[piv + (long long)col * lda] = x;
         }
         __syncthreads();
 #pragma unroll
@@ -255,33 +253,88 @@ __global__ void __launch_bounds__(LP_THREADS) lu_panel_reg_kernel(int n, int j0,
 #pragma unroll
         for (int c = 0; c < LP_SB; ++c)
           if (c < sb) st2(&A[r + (long long)(c0 + c) * lda], v[k][c]);
+      if (r < c0 + sb)  // the unit-lower diagonal block L11, for U12 below
+#pragma unroll
+        for (int c = 0; c < LP_SB; ++c) s_l11[r - c0][c] = v[k][c];
     }
     const int rest = j0 + jb - (c0 + sb);  // panel columns right of the sub-panel
     if (rest > 0) {
       __syncthreads();
-      // U12 = L11^-1 A12 (unit lower L11 = sub-panel rows c0..c0+sb-1)
+      // one thread per column to the right: the sub-panel's row swaps (the
+      // rows c0.. and the pivot rows gathered into registers, swapped, stored
+      // back), then U12 = L11^-1 A12 on the swapped values; the panel's columns
+      // to the left get these swaps from the laswp launch after the panel
       if (tid < rest) {
         const int col = c0 + sb + tid;
-        for (int i = 0; i < sb; ++i) {
-          cplx u = ld2(&A[c0 + i + (long long)col * lda]);
-          for (int q = 0; q < i; ++q) u = u - ld2(&A[c0 + i + (long long)(c0 + q) * lda]) * s_u12[q][tid];
-          s_u12[i][tid] = u;
-          st2(&A[c0 + i + (long long)col * lda], u);
+        double2* Ac = A + (long long)col * lda;
+        int rows[2 * LP_SB];
+        cplx val[2 * LP_SB];
+        int nr = 0;
+#pragma unroll
+        for (int i = 0; i < LP_SB; ++i)
+          if (i < sb) rows[nr++] = c0 + i;
+#pragma unroll
+        for (int c = 0; c < LP_SB; ++c) {
+          if (c < sb) {
+            const int pr = s_pivs[c];
+            bool seen = false;
+            for (int t = 0; t < nr; ++t) seen |= (rows[t] == pr);
+            if (!seen) rows[nr++] = pr;
+          }
         }
+        for (int t = 0; t < nr; ++t) val[t] = ld2(&Ac[rows[t]]);
+#pragma unroll
+        for (int c = 0; c < LP_SB; ++c) {
+          if (c < sb) {
+            const int pr = s_pivs[c];
+            if (pr != c0 + c) {
+              int ia = 0, ib = 0;
+              for (int t = 0; t < nr; ++t) {
+                if (rows[t] == c0 + c) ia = t;
+                if (rows[t] == pr) ib = t;
+              }
+              const cplx x = val[ia];
+              val[ia] = val[ib];
+              val[ib] = x;
+            }
+          }
+        }
+        // rows c0..c0+sb-1 are val[0..sb-1]: forward substitution with L11
+#pragma unroll
+        for (int i = 0; i < LP_SB; ++i) {
+          if (i < sb) {
+            cplx u = val[i];
+#pragma unroll
+            for (int q = 0; q < LP_SB; ++q)
+              if (q < i) u = u - s_l11[i][q] * s_u12[q][tid];
+            s_u12[i][tid] = u;
+            val[i] = u;
+          }
+        }
+        for (int t = 0; t < nr; ++t) st2(&Ac[rows[t]], val[t]);
       }
       __syncthreads();
-      // A22 -= L21 U12 for rows below the sub-panel (L21 in registers)
+      // A22 -= L21 U12 for rows below the sub-panel (L21 in registers), eight
+      // columns at a time with every load issued before the stores
 #pragma unroll
       for (int k = 0; k < RPT; ++k) {
         const int r = c0 + tid + k * LP_THREADS;
         if (r >= c0 + sb && r < n) {
-          for (int j = 0; j < rest; ++j) {
-            double2* p = &A[r + (long long)(c0 + sb + j) * lda];
-            cplx acc = ld2(p);
+          for (int j0b = 0; j0b < rest; j0b += 8) {
+            cplx a8[8];
 #pragma unroll
-            for (int q = 0; q < LP_SB; ++q)
-              if (q < sb) acc = acc - v[k][q] * s_u12[q][j];
-            st2(p, acc);
+            for (int j = 0; j < 8; ++j)
+              if (j0b + j < rest) a8[j] = ld2(&A[r + (long long)(c0 + sb + j0b + j) * lda]);
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+              if (j0b + j < rest) {
+                cplx acc = a8[j];
+#pragma unroll
+                for (int q = 0; q < LP_SB; ++q)
+                  if (q < sb) acc = acc - v[k][q] * s_u12[q][j0b + j];
+                st2(&A[r + (long long)(c0 + sb + j0b + j) * lda], acc);
+              }
+            }
           }
         }
       }
@@ -291,15 +344,24 @@ __global__ void __launch_bounds__(LP_THREADS) lu_panel_reg_kernel(int n, int j0,
 }
 
 // Row swaps ipiv[j0..j0+jb) applied to every column outside [skip0, skip1).
+// Columns in [skip0, skip1) (the panel's own) are skipped when sub == 0; with
+// sub > 0 the panel was factored sub columns at a time and already applied to
+// each of its columns the swaps up to the end of that column's sub-panel, so
+// only the later ones remain.
 __global__ void lu_laswp_kernel(int n, int ncols, int j0, int jb, int skip0, int skip1,
                                 double2* A, long long lda, long long sa, const int* ipiv,
-                                long long ipiv_stride) {
+                                long long ipiv_stride, int sub) {
   const int b = blockIdx.y;
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= ncols || (c >= skip0 && c < skip1)) return;
+  if (c >= ncols) return;
+  int first = j0;
+  if (c >= skip0 && c < skip1) {
+    if (sub <= 0) return;
+    first = skip0 + ((c - skip0) / sub + 1) * sub;
+  }
   A += (long long)b * sa;
   ipiv += (long long)b * ipiv_stride;
-  for (int jj = j0; jj < j0 + jb; ++jj) {
+  for (int jj = first; jj < j0 + jb; ++jj) {
     int p = ipiv[jj];
     if (p != jj) {
       double2 t = A[jj + (long long)c * lda];
@@ -380,7 +442,8 @@ int lu_factor(int n, double2* A, long long lda, long long sa, int* ipiv, int* in
       lu_panel_kernel<<<batch, LU_PANEL_THREADS, 0, stream>>>(n, j0, jb, A, lda, sa, ipiv, info);
     EUV_LAUNCH_CHECK();
     dim3 gs((n + 127) / 128, batch);
-    lu_laswp_kernel<<<gs, 128, 0, stream>>>(n, n, j0, jb, j0, j0 + jb, A, lda, sa, ipiv, n);
+    lu_laswp_kernel<<<gs, 128, 0, stream>>>(n, n, j0, jb, j0, j0 + jb, A, lda, sa, ipiv, n,
+                                            n <= 4 * LP_THREADS ? LP_SB : 0);
     EUV_LAUNCH_CHECK();
     const int rest = n - j0 - jb;
     if (rest > 0) {
@@ -594,7 +657,7 @@ int lu_solve(int n, int nrhs, const double2* LU, long long lda, long long sa, co
              double2* B, long long ldb, long long sb, int batch, cudaStream_t stream) {
   if (n <= 0 || nrhs <= 0 || batch <= 0) return EUV_OK;
   dim3 gs((nrhs + 127) / 128, batch);
-  lu_laswp_kernel<<<gs, 128, 0, stream>>>(n, nrhs, 0, n, 0, 0, B, ldb, sb, ipiv, n);
+  lu_laswp_kernel<<<gs, 128, 0, stream>>>(n, nrhs, 0, n, 0, 0, B, ldb, sb, ipiv, n, 0);
   EUV_LAUNCH_CHECK();
   if (batch <= 65535) {
     const size_t col = (size_t)n * sizeof(double2);
