@@ -174,11 +174,25 @@ __global__ void __launch_bounds__(MX_THREADS, 1)
 
   if (p.steps != nullptr && p.step >= p.steps[b]) {
     // inactive double-angle step of this batch entry: C = A on this tile
+    // (eight loads in flight per thread before their stores: the CTA holds a
+    // whole SM's shared memory, so the copy must not wait on each element)
     const double2* A = p.a + (long long)b * p.sa;
-    for (int idx = threadIdx.x; idx < MX_BM * MX_BN; idx += MX_THREADS) {
-      int i = idx % MX_BM, j = idx / MX_BM;
-      int gi = m0 + i, gj = n0 + j;
-      if (gi < p.m && gj < p.n) C[gi + (long long)gj * p.ldc] = A[gi + (long long)gj * p.lda];
+    constexpr int U = 8;
+    for (int base = 0; base < MX_BM * MX_BN; base += MX_THREADS * U) {
+      double2 v[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int idx = base + threadIdx.x + u * MX_THREADS;
+        const int gi = m0 + idx % MX_BM, gj = n0 + idx / MX_BM;
+        v[u] = (idx < MX_BM * MX_BN && gi < p.m && gj < p.n) ? A[gi + (long long)gj * p.lda]
+                                                             : make_double2(0.0, 0.0);
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int idx = base + threadIdx.x + u * MX_THREADS;
+        const int gi = m0 + idx % MX_BM, gj = n0 + idx / MX_BM;
+        if (idx < MX_BM * MX_BN && gi < p.m && gj < p.n) C[gi + (long long)gj * p.ldc] = v[u];
+      }
     }
     return;
   }

@@ -68,10 +68,23 @@ __global__ void __launch_bounds__(GTHREADS, 2) zgemm_kernel(GemmArgs p) {
 
   if (p.steps != nullptr && p.step >= p.steps[bz]) {
     // inactive double-angle step for this batch entry: C = A
-    for (int idx = tid; idx < GBM * GBN; idx += GTHREADS) {
-      int i = idx % GBM, j = idx / GBM;
-      int gi = m0 + i, gj = n0 + j;
-      if (gi < p.m && gj < p.n) C[gi + (long long)gj * p.ldc] = A[gi + (long long)gj * p.lda];
+    // eight loads in flight per thread before their stores
+    constexpr int U = 8;
+    for (int base = 0; base < GBM * GBN; base += GTHREADS * U) {
+      double2 v[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int idx = base + tid + u * GTHREADS;
+        const int gi = m0 + idx % GBM, gj = n0 + idx / GBM;
+        v[u] = (idx < GBM * GBN && gi < p.m && gj < p.n) ? A[gi + (long long)gj * p.lda]
+                                                         : make_double2(0.0, 0.0);
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int idx = base + tid + u * GTHREADS;
+        const int gi = m0 + idx % GBM, gj = n0 + idx / GBM;
+        if (idx < GBM * GBN && gi < p.m && gj < p.n) C[gi + (long long)gj * p.ldc] = v[u];
+      }
     }
     return;
   }
