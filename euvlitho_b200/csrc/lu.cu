@@ -139,7 +139,7 @@ __global__ void __launch_bounds__(LP_THREADS) lu_panel_reg_kernel(int n, int j0,
   __shared__ double red_v[LP_THREADS / 32];
   __shared__ int red_i[LP_THREADS / 32];
   __shared__ int s_piv;
-  __shared__ cplx s_rowa[LP_SB], s_rowb[LP_SB], s_prow[LP_SB];
+  __shared__ cplx s_rowa[LP_SB], s_prow[LP_SB];
   __shared__ cplx s_u12[LP_SB][LU_NB];
   __shared__ cplx s_l11[LP_SB][LP_SB];
   __shared__ int s_pivs[LP_SB];
@@ -185,50 +185,50 @@ __global__ void __launch_bounds__(LP_THREADS) lu_panel_reg_kernel(int n, int j0,
         red_i[warp] = bidx;
       }
       __syncthreads();
-      if (tid == 0) {
-        double bv = red_v[0];
-        int bi = red_i[0];
-        for (int w = 1; w < LP_THREADS / 32; ++w)
-          if (red_v[w] > bv || (red_v[w] == bv && red_i[w] < bi)) {
-            bv = red_v[w];
-            bi = red_i[w];
+      if (warp == 0) {  // the warp maxima, same rule (first index of the maximum)
+        double bv = lane < LP_THREADS / 32 ? red_v[lane] : -1.0;
+        int bi = lane < LP_THREADS / 32 ? red_i[lane] : n;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+          const double ov = __shfl_down_sync(0xffffffffu, bv, off);
+          const int oi = __shfl_down_sync(0xffffffffu, bi, off);
+          if (ov > bv || (ov == bv && oi < bi)) {
+            bv = ov;
+            bi = oi;
           }
-        if (bi >= n) bi = jj;
-        s_piv = bi;
-        s_pivs[c] = bi;
-        ipiv[jj] = bi;
+        }
+        if (lane == 0) {
+          if (bi >= n) bi = jj;
+          s_piv = bi;
+          s_pivs[c] = bi;
+          ipiv[jj] = bi;
+        }
       }
       __syncthreads();
       const int piv = s_piv;
+      // one exchange through shared memory: the new row jj (= old row piv) is
+      // also the pivot row the update below broadcasts
+#pragma unroll
+      for (int k = 0; k < RPT; ++k) {
+        const int r = c0 + tid + k * LP_THREADS;
+#pragma unroll
+        for (int cc = 0; cc < LP_SB; ++cc) {
+          if (r == piv) s_prow[cc] = v[k][cc];
+          if (r == jj) s_rowa[cc] = v[k][cc];
+        }
+      }
+      __syncthreads();
       if (piv != jj) {
 #pragma unroll
         for (int k = 0; k < RPT; ++k) {
           const int r = c0 + tid + k * LP_THREADS;
 #pragma unroll
           for (int cc = 0; cc < LP_SB; ++cc) {
-            if (r == jj) s_rowa[cc] = v[k][cc];
-            if (r == piv) s_rowb[cc] = v[k][cc];
-          }
-        }
-        __syncthreads();
-#pragma unroll
-        for (int k = 0; k < RPT; ++k) {
-          const int r = c0 + tid + k * LP_THREADS;
-#pragma unroll
-          for (int cc = 0; cc < LP_SB; ++cc) {
-            if (r == jj) v[k][cc] = s_rowb[cc];
+            if (r == jj) v[k][cc] = s_prow[cc];
             if (r == piv) v[k][cc] = s_rowa[cc];
           }
         }
       }
-#pragma unroll
-      for (int k = 0; k < RPT; ++k) {
-        const int r = c0 + tid + k * LP_THREADS;
-        if (r == jj)
-#pragma unroll
-          for (int cc = 0; cc < LP_SB; ++cc) s_prow[cc] = v[k][cc];
-      }
-      __syncthreads();
       const cplx d = s_prow[c];
       if (d.x == 0.0 && d.y == 0.0) {
         if (tid == 0 && info[blockIdx.x] == 0) info[blockIdx.x] = jj + 1;

@@ -468,15 +468,32 @@ class Plan:
 
 
     # ------------------------------------------------------------ STCC-SOCS
+    def socs_padding(self) -> Tuple[int, int]:
+        """(index of the (0,0) pupil point, its extra copies) in the reference's
+        TCC: eigenfunction.py:60-66 takes ncut = len(linput) from
+        find_valid_pupil_points, whose arrays have the wide order count (rounded
+        diamond, cut 6) with the unused tail at (0,0)."""
+        L_, M_ = self.cfg.order_limits("diamond", 6.0)
+        nrange = len(T.order_set("diamond", L_, M_)[0])
+        z = int(np.nonzero((self.linput == 0) & (self.minput == 0))[0][0])
+        return z, max(0, nrange - self.ncut)
+
     def socs_tables(self, z: Optional[float] = None, nsocs: int = 100, nsocsxy: int = 20,
-                    nout: int = 64, mesh_deg: float = 0.2, max_sweeps: int = 30):
+                    nout: int = 64, mesh_deg: float = 0.2, max_sweeps: int = 30,
+                    reference_padding: bool = True):
         """Resident SOCS kernels (eigenfunction.py:5-163): the three TCC
         matrices over the linear model's source grid as device GEMMs, their
         eigenpairs by the device Jacobi solver (euv_heev), the nsocs / nsocsxy
-        kernels of largest |alpha|, and the DFT / interpolation tables."""
+        kernels of largest |alpha|, and the DFT / interpolation tables.
+
+        ``reference_padding``: reproduce the reference's TCC, which repeats the
+        (0,0) pupil point d more times (``socs_padding``).  Its nonzero spectrum
+        is that of D^1/2 T D^1/2, D = I + d e_z e_z^T, and its eigenvectors on the
+        pupil points are those of D^1/2 T D^1/2 with component z divided by
+        sqrt(1 + d): the same result from an ncut-size problem."""
         cfg = self.cfg
         z = float(cfg.z if z is None else z)
-        key = (z, nsocs, nsocsxy, nout, mesh_deg)
+        key = (z, nsocs, nsocsxy, nout, mesh_deg, reference_padding)
         tb = getattr(self, "_socs_tables", None)
         if tb is not None and tb["key"] == key:
             return tb
@@ -492,6 +509,8 @@ class Plan:
         lib = L.lib()
         wb = lib.euv_heev_workspace_bytes(n)
         hw = torch.empty(wb, dtype=torch.uint8, device=dev)
+        iz, pad_copies = self.socs_padding() if reference_padding else (0, 0)
+        pad_scale = math.sqrt(1.0 + pad_copies)
         out = {}
         for name, wt in (("s0", np.ones(S)), ("sx", dsx), ("sy", dsy)):
             q = torch.from_numpy(np.conj(pall) * np.tile(wt * w0, 3)[None, :]).to(dev)  # col-major 3S x n
@@ -500,11 +519,16 @@ class Plan:
                    q.data_ptr(), 3 * S, 0, L.c64.of(0), tcc.data_ptr(), n, 0, L.c64.of(0), 1,
                    None, 0, _stream())
             del q
+            if pad_copies:  # column-major: tcc[j][i] = TCC(i, j)
+                tcc[iz, :] *= pad_scale
+                tcc[:, iz] *= pad_scale
             w = torch.empty(n, dtype=torch.float64, device=dev)
             v = torch.empty((n, n), dtype=torch.complex128, device=dev)
             L.call("euv_heev", n, tcc.data_ptr(), n, w.data_ptr(), v.data_ptr(), n, max_sweeps,
                    1e-14, hw.data_ptr(), wb, self.status.data_ptr(), _stream())
             self.check()
+            if pad_copies:  # v[j][i] = component i of eigenvector j
+                v[:, iz] /= pad_scale
             wh = w.cpu().numpy()
             order = np.lexsort((wh, -np.abs(wh)))   # |alpha| descending, ties ascending
             keep = nsocs if name == "s0" else nsocsxy

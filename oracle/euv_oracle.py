@@ -1016,11 +1016,36 @@ def socs_tcc(cfg: SimConfig, z: float = 0.0, mesh_deg: float = 0.2):
     return tuple(out)
 
 
-def socs_eigen(tcc):
+def socs_padding(cfg: SimConfig):
+    """(index of the (0,0) pupil point, its extra copies) of the reference's TCC:
+    eigenfunction.py:60-66 takes ncut = len(linput) from find_valid_pupil_points,
+    whose arrays have the wide order count (rounded diamond, cut 6) with the
+    unused tail left at (0,0) -- so the TCC runs over the pupil points plus
+    Nrange - ncut copies of the (0,0) point."""
+    lin, mn, _, _ = pupil_set(cfg)
+    L_, M_ = order_limits(cfg, "diamond", 6.0)
+    nrange = len(order_set("diamond", L_, M_)[0])
+    z = int(np.nonzero((lin == 0) & (mn == 0))[0][0])
+    return z, nrange - len(lin)
+
+
+def socs_eigen(tcc, z=None, copies=0):
     """Eigenpairs of one TCC sorted by |alpha|, largest first, ties in
     ascending-eigenvalue order (eigenfunction.py:125-163).  Returns (alpha,
-    phi) with phi[m] the m-th eigenvector."""
-    w, v = np.linalg.eigh(tcc)
+    phi) with phi[m] the m-th eigenvector on the pupil points.
+
+    With ``copies`` > 0, the eigenpairs of the padded TCC M T M^H (point z
+    repeated ``copies`` more times) restricted to the pupil points: its nonzero
+    spectrum is that of D^1/2 T D^1/2 with D = I + copies e_z e_z^T, and the
+    eigenvector on the pupil points is y with y_z / sqrt(1 + copies)."""
+    t = np.array(tcc, copy=True)
+    if copies:
+        sc = np.sqrt(1.0 + copies)
+        t[z, :] *= sc
+        t[:, z] *= sc
+    w, v = np.linalg.eigh(t)
+    if copies:
+        v[z, :] /= sc
     order = np.argsort(-np.abs(w), kind="stable")
     return w[order], v[:, order].T.copy()
 

@@ -71,11 +71,14 @@ def test_socs_image_matches_the_oracle(cuda):
     cfg = SimConfig(ndivx=512, ndivy=512)
     plan = Plan(cfg, device=cuda)
     tb = plan.socs_tables(nsocs=60, nsocsxy=12)
-    tcc = O.socs_tcc(to_oracle(cfg), 0.0)
+    oc = to_oracle(cfg)
+    tcc = O.socs_tcc(oc, 0.0)
+    z, copies = O.socs_padding(oc)
+    assert (z, copies) == plan.socs_padding()
     for t, name in zip(tcc, ("s0", "sx", "sy")):
         # TCC_sx / TCC_sy have +-lambda pairs (the source grid is symmetric):
         # their order within |alpha| ties is set by rounding, so compare spectra
-        lam = np.linalg.eigvalsh(t)
+        lam = np.sort(O.socs_eigen(t, z, copies)[0])
         got = np.sort(tb["eig_" + name])
         assert np.max(np.abs(got - lam)) < 1e-12 * np.max(np.abs(lam)), name
     rng = np.random.default_rng(3)

@@ -24,7 +24,8 @@ def golden():
 def eig():
     cfg = O.SimConfig()
     tccs = O.socs_tcc(cfg, 0.0)
-    return cfg, [O.socs_eigen(t) for t in tccs]
+    z, copies = O.socs_padding(cfg)  # the reference's padded pupil list
+    return cfg, [O.socs_eigen(t, z, copies) for t in tccs]
 
 
 def test_tcc_eigenvalues_match_the_reference(golden, eig):
