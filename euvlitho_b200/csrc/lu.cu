@@ -11,7 +11,9 @@
 //            the panel, scale, rank-1 update), sub-panels in registers;
 //   laswp  : the panel's row swaps applied to the other columns;
 //   trsm   : U12 = L11^-1 A12 (unit lower, L11 staged in shared memory);
-//   update : A22 -= L21 U12 with the batched DMMA zgemm.
+//   update : A22 -= L21 U12 with the batched DMMA zgemm;
+//   look-ahead: the next panel is factored on a high-priority side stream while
+//            the rest of the update runs (the panel alone fills only `batch` SMs).
 // Solve: the row swaps on B, then one launch that keeps 8 (or fewer, for large
 // n) columns of X in shared memory per CTA through both substitutions.
 #include "common.cuh"
@@ -425,39 +427,96 @@ __global__ void zero_int_kernel(int* p, int n) {
   if (i < n) p[i] = 0;
 }
 
+// Side stream (highest priority) and fork/join events of the look-ahead, one
+// set per host thread and device, created by the first call (which therefore
+// has to come before any stream capture).
+struct LuSide {
+  cudaStream_t hi = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+};
+static cudaError_t lu_side(LuSide** out) {
+  static thread_local LuSide per_dev[64];
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  LuSide& s = per_dev[dev];
+  if (s.hi == nullptr) {
+    int lo = 0, hi = 0;
+    if ((e = cudaDeviceGetStreamPriorityRange(&lo, &hi)) != cudaSuccess) return e;
+    if ((e = cudaStreamCreateWithPriority(&s.hi, cudaStreamNonBlocking, hi)) != cudaSuccess) return e;
+    if ((e = cudaEventCreateWithFlags(&s.fork, cudaEventDisableTiming)) != cudaSuccess) return e;
+    if ((e = cudaEventCreateWithFlags(&s.join, cudaEventDisableTiming)) != cudaSuccess) return e;
+  }
+  *out = &s;
+  return cudaSuccess;
+}
+
+static int lu_panel(int n, int j0, int jb, double2* A, long long lda, long long sa, int* ipiv,
+                    int* info, int batch, cudaStream_t st) {
+  if (n <= LP_THREADS)
+    lu_panel_reg_kernel<1><<<batch, LP_THREADS, 0, st>>>(n, j0, jb, A, lda, sa, ipiv, info);
+  else if (n <= 2 * LP_THREADS)
+    lu_panel_reg_kernel<2><<<batch, LP_THREADS, 0, st>>>(n, j0, jb, A, lda, sa, ipiv, info);
+  else if (n <= 4 * LP_THREADS)
+    lu_panel_reg_kernel<4><<<batch, LP_THREADS, 0, st>>>(n, j0, jb, A, lda, sa, ipiv, info);
+  else
+    lu_panel_kernel<<<batch, LU_PANEL_THREADS, 0, st>>>(n, j0, jb, A, lda, sa, ipiv, info);
+  EUV_LAUNCH_CHECK();
+  return EUV_OK;
+}
+
+// U12 = L11^-1 A12 and A22 -= L21 U12 of panel [j0, j0+jb) for the columns
+// [c0, c0+nc) (rows j0.. of the factor).
+static int lu_update(int n, int j0, int jb, int c0, int nc, double2* A, long long lda,
+                     long long sa, int batch, cudaStream_t st) {
+  if (nc <= 0) return EUV_OK;
+  dim3 gt((nc + 127) / 128, batch);
+  lu_trsm_block_kernel<<<gt, 128, 0, st>>>(jb, nc, 1, A + j0 + (long long)j0 * lda, lda, sa,
+                                           A + j0 + (long long)c0 * lda, lda, sa);
+  EUV_LAUNCH_CHECK();
+  const int rest = n - j0 - jb;
+  return zgemm(rest, nc, jb, mk(-1.0, 0.0), nullptr, A + (j0 + jb) + (long long)j0 * lda, lda, sa,
+               A + j0 + (long long)c0 * lda, lda, sa, mk(1.0, 0.0),
+               A + (j0 + jb) + (long long)c0 * lda, lda, sa, mk(0.0, 0.0), batch, nullptr, 0, st);
+}
+
+// Right-looking LU with one panel of look-ahead: after panel j, its update of
+// the next panel's columns runs first; then the next panel is factored on the
+// high-priority side stream (its batch CTAs take SMs as soon as any frees up)
+// while the update of the remaining columns runs on the caller's stream.  The
+// column sets are disjoint; the laswp of the next panel waits for both.
 int lu_factor(int n, double2* A, long long lda, long long sa, int* ipiv, int* info, int batch,
               cudaStream_t stream) {
   if (n <= 0 || batch <= 0) return EUV_OK;
+  LuSide* side = nullptr;
+  EUV_CUDA_TRY(lu_side(&side));
   zero_int_kernel<<<(batch + 255) / 256, 256, 0, stream>>>(info, batch);
   EUV_LAUNCH_CHECK();
-  for (int j0 = 0; j0 < n; j0 += LU_NB) {
-    const int jb = (n - j0) < LU_NB ? (n - j0) : LU_NB;
-    if (n <= LP_THREADS)
-      lu_panel_reg_kernel<1><<<batch, LP_THREADS, 0, stream>>>(n, j0, jb, A, lda, sa, ipiv, info);
-    else if (n <= 2 * LP_THREADS)
-      lu_panel_reg_kernel<2><<<batch, LP_THREADS, 0, stream>>>(n, j0, jb, A, lda, sa, ipiv, info);
-    else if (n <= 4 * LP_THREADS)
-      lu_panel_reg_kernel<4><<<batch, LP_THREADS, 0, stream>>>(n, j0, jb, A, lda, sa, ipiv, info);
-    else
-      lu_panel_kernel<<<batch, LU_PANEL_THREADS, 0, stream>>>(n, j0, jb, A, lda, sa, ipiv, info);
-    EUV_LAUNCH_CHECK();
+  const int sub = n <= 4 * LP_THREADS ? LP_SB : 0;
+  int j0 = 0, jb = n < LU_NB ? n : LU_NB;
+  int rc = lu_panel(n, j0, jb, A, lda, sa, ipiv, info, batch, stream);
+  if (rc) return rc;
+  for (;;) {
     dim3 gs((n + 127) / 128, batch);
-    lu_laswp_kernel<<<gs, 128, 0, stream>>>(n, n, j0, jb, j0, j0 + jb, A, lda, sa, ipiv, n,
-                                            n <= 4 * LP_THREADS ? LP_SB : 0);
+    lu_laswp_kernel<<<gs, 128, 0, stream>>>(n, n, j0, jb, j0, j0 + jb, A, lda, sa, ipiv, n, sub);
     EUV_LAUNCH_CHECK();
     const int rest = n - j0 - jb;
-    if (rest > 0) {
-      dim3 gt((rest + 127) / 128, batch);
-      lu_trsm_block_kernel<<<gt, 128, 0, stream>>>(jb, rest, 1, A + j0 + (long long)j0 * lda,
-                                                    lda, sa, A + j0 + (long long)(j0 + jb) * lda,
-                                                    lda, sa);
-      EUV_LAUNCH_CHECK();
-      int rc = zgemm(rest, rest, jb, mk(-1.0, 0.0), nullptr, A + (j0 + jb) + (long long)j0 * lda,
-                     lda, sa, A + j0 + (long long)(j0 + jb) * lda, lda, sa, mk(1.0, 0.0),
-                     A + (j0 + jb) + (long long)(j0 + jb) * lda, lda, sa, mk(0.0, 0.0), batch,
-                     nullptr, 0, stream);
-      if (rc != EUV_OK) return rc;
+    if (rest <= 0) break;
+    const int j1 = j0 + jb, nb2 = rest < LU_NB ? rest : LU_NB, rem = rest - nb2;
+    if ((rc = lu_update(n, j0, jb, j1, nb2, A, lda, sa, batch, stream))) return rc;
+    if (rem > 0) {
+      EUV_CUDA_TRY(cudaEventRecord(side->fork, stream));
+      EUV_CUDA_TRY(cudaStreamWaitEvent(side->hi, side->fork, 0));
+      if ((rc = lu_panel(n, j1, nb2, A, lda, sa, ipiv, info, batch, side->hi))) return rc;
+      if ((rc = lu_update(n, j0, jb, j1 + nb2, rem, A, lda, sa, batch, stream))) return rc;
+      EUV_CUDA_TRY(cudaEventRecord(side->join, side->hi));
+      EUV_CUDA_TRY(cudaStreamWaitEvent(stream, side->join, 0));
+    } else if ((rc = lu_panel(n, j1, nb2, A, lda, sa, ipiv, info, batch, stream))) {
+      return rc;
     }
+    j0 = j1;
+    jb = nb2;
   }
   return EUV_OK;
 }
