@@ -472,7 +472,7 @@ int gemm_mixed(int m, int n, int k, cplx alpha, const double* scale, const doubl
                long long lda, long long sa, const double2* b, long long ldb, long long sb,
                cplx beta, double2* c, long long ldc, long long sc, cplx diag, int batch,
                const int* steps, int step, void* work, size_t work_bytes, int* status,
-               cudaStream_t stream) {
+               cudaStream_t stream, int reuse) {
   if (m <= 0 || n <= 0 || batch <= 0) return EUV_OK;
   if (k <= 0 || batch > 65535 || (size_t)batch * MX_PLANES > 0x7fffffff) {
     euv_set_error("gemm_mixed: unsupported shape");
@@ -496,10 +496,15 @@ int gemm_mixed(int m, int n, int k, cplx alpha, const double* scale, const doubl
     err = reinterpret_cast<int*>(w + abytes + bbytes);
     EUV_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int), stream));
   }
-  {
+  // reuse bit 0 / bit 1: the A / B planes in this workspace are already those
+  // of the operand (the caller's previous call split the same unchanged
+  // matrix in the same role and shape), so the split is skipped
+  if (!(reuse & 1)) {
     dim3 g((m + 31) / 32, (kp + 31) / 32, batch), t(32, 8);
     split_a_kernel<<<g, t, 0, stream>>>(m, k, kp, a, lda, sa, pa, steps, step);
     EUV_LAUNCH_CHECK();
+  }
+  if (!(reuse & 2)) {
     dim3 gb((unsigned)(((long long)n * kp + 255) / 256), batch);
     split_b_kernel<<<gb, 256, 0, stream>>>(k, n, kp, b, ldb, sb, pb, steps, step);
     EUV_LAUNCH_CHECK();
@@ -557,5 +562,5 @@ extern "C" int euv_zgemm_tf32x3(int m, int n, int k, euv_c64 alpha, const double
   return gemm_mixed(m, n, k, fromc(alpha), d_scale, reinterpret_cast<const double2*>(d_a), lda,
                     stride_a, reinterpret_cast<const double2*>(d_b), ldb, stride_b, fromc(beta),
                     reinterpret_cast<double2*>(d_c), ldc, stride_c, fromc(diag), batch, d_steps,
-                    step, d_work, work_bytes, d_status, (cudaStream_t)stream);
+                    step, d_work, work_bytes, d_status, (cudaStream_t)stream, 0);
 }
