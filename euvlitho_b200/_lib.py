@@ -38,6 +38,8 @@ EXPORTS = (
     "euv_matfun_workspace_bytes", "euv_matfun_cs", "euv_matfun_cs_noalloc",
     "euv_wait_probe", "euv_linear_amp", "euv_mask_raster_workspace_bytes", "euv_mask_raster",
     "euv_heev_workspace_bytes", "euv_heev", "euv_socs_workspace_bytes", "euv_socs_image",
+    "euv_cnn_blob_bytes", "euv_cnn_pack", "euv_cnn_workspace_bytes", "euv_cnn_predict",
+    "euv_cnn_downsample",
 )
 
 
@@ -133,6 +135,25 @@ class SocsDesc(C.Structure):
     ]
 
 
+EUV_CNN_MAX_MODELS = 6
+EUV_CNN_MAX_OUT = 8192
+
+
+class CnnModelWeights(C.Structure):
+    _fields_ = [
+        ("conv_w", P * 5), ("conv_b", P * 5), ("bn_w", P * 5), ("bn_b", P * 5),
+        ("bn_mean", P * 5), ("bn_var", P * 5),
+        ("fc1_w", P), ("fc1_b", P), ("fc2_w", P), ("fc2_b", P), ("n_out", C.c_int),
+    ]
+
+
+class CnnDesc(C.Structure):
+    _fields_ = [
+        ("n_models", C.c_int), ("n_masks", C.c_int), ("max_out", C.c_int),
+        ("n_out", C.c_int * EUV_CNN_MAX_MODELS), ("d_factors", P), ("d_status", P),
+    ]
+
+
 _lib: Optional[C.CDLL] = None
 
 
@@ -188,6 +209,16 @@ def _declare(lib: C.CDLL) -> None:
     lib.euv_mask_raster.argtypes = [i, i, i, i, P, i, P, P, P, sz, P]
     lib.euv_linear_amp.argtypes = [C.POINTER(LinearDesc), P, P, P, P, P, P]
     lib.euv_wait_probe.argtypes = [P, ll, P, P]
+    lib.euv_cnn_blob_bytes.restype = sz
+    lib.euv_cnn_blob_bytes.argtypes = [i, i]
+    lib.euv_cnn_pack.restype = i
+    lib.euv_cnn_pack.argtypes = [i, C.POINTER(CnnModelWeights), i, d, P, sz, P]
+    lib.euv_cnn_workspace_bytes.restype = sz
+    lib.euv_cnn_workspace_bytes.argtypes = [i, i, i]
+    lib.euv_cnn_predict.restype = i
+    lib.euv_cnn_predict.argtypes = [C.POINTER(CnnDesc), P, P, P, P, sz, P]
+    lib.euv_cnn_downsample.restype = i
+    lib.euv_cnn_downsample.argtypes = [i, P, P, P]
 
 
 def lib() -> C.CDLL:

@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libeuvl_b200.so")
-SOURCES = ["api.cu", "zgemm.cu", "lu.cu", "rcwa.cu", "abbe.cu", "m3d.cu", "gemm_mixed.cu", "linear.cu", "raster.cu", "jacobi.cu", "socs.cu"]
+SOURCES = ["api.cu", "zgemm.cu", "lu.cu", "rcwa.cu", "abbe.cu", "m3d.cu", "gemm_mixed.cu", "linear.cu", "raster.cu", "jacobi.cu", "socs.cu", "cnn.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -30,7 +30,8 @@ def nvcc_path() -> str:
 
 def build(verbose: bool = False, ptxas_info: bool = False, force: bool = False) -> str:
     srcs = [os.path.join(CSRC, s) for s in SOURCES]
-    deps = srcs + [os.path.join(CSRC, "common.cuh"), os.path.join(ROOT, "include", "euvl_b200.h")]
+    deps = srcs + [os.path.join(CSRC, h) for h in sorted(os.listdir(CSRC)) if h.endswith(".cuh")]
+    deps.append(os.path.join(ROOT, "include", "euvl_b200.h"))
     if (not force and os.path.exists(LIB)
             and os.path.getmtime(LIB) >= max(os.path.getmtime(d) for d in deps)):
         return LIB

@@ -4,6 +4,7 @@
   python -m euvlitho_b200.cli m3d         # m3d.out: ./mask.bin -> inputxx.csv, inputlm.csv
   python -m euvlitho_b200.cli linear      # linear.py: ./mask.bin + inputxx.csv -> intlinear.csv, intft.csv
   python -m euvlitho_b200.cli maskgen     # mask.out: mask.bin (--count masks) + maskimage.csv
+  python -m euvlitho_b200.cli predict --models DIR   # predict.py: ./mask.bin -> inputxx.csv
 
 Both run the reference configuration (intensity.cpp:44-91, m3d.cpp:34-95) on
 the GPU; --preset picks another workload.
@@ -24,7 +25,9 @@ from .engine import Plan
 
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("what", choices=["intensity", "m3d", "linear", "maskgen"])
+    ap.add_argument("what", choices=["intensity", "m3d", "linear", "maskgen", "predict"])
+    ap.add_argument("--models", default="../model",
+                    help="predict: directory with re0/ im0/ rex/ imx/ rey/ imy/ model.ckpt and factors")
     ap.add_argument("--seed", type=int, default=1, help="srand seed (maskgen; 1 = the reference's)")
     ap.add_argument("--inputxx", default="./inputxx.csv", help="M3D parameters (linear)")
     ap.add_argument("--preset", default="reference")
@@ -44,6 +47,14 @@ def main(argv=None) -> int:
             for row in first:
                 fh.write("".join("%d," % v for v in row))
                 fh.write("\n")
+        print("elapsed time (s) %.3f" % (time.time() - t0))
+        return 0
+    if a.what == "predict":
+        from . import cnn
+        pred = cnn.CnnPredictor.from_checkpoints(a.models)       # predict.py:123-131
+        raw = np.fromfile(a.mask, np.uint8)
+        outs = pred.predict(raw.reshape(-1, cnn.MASK_BYTES))     # predict.py:133-142
+        cnn.write_inputxx("inputxx.csv", outs)                   # predict.py:145-151
         print("elapsed time (s) %.3f" % (time.time() - t0))
         return 0
     plan = Plan(cfg, precision=a.precision, pols=(a.pol,))

@@ -25,8 +25,7 @@
 //                FP64 result written column by column (coalesced).
 // All waits are bounded (about 2 s); a timeout ORs EUV_STATUS_TIMEOUT into the
 // status word, drains the copies and MMAs in flight, frees TMEM and returns.
-#include <cuda.h>
-#include "common.cuh"
+#include "tcgen05.cuh"
 
 namespace euv {
 
@@ -61,98 +60,12 @@ struct MixedArgs {
   int* err;
 };
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
-               "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// Bounded wait: false after the deadline (the status word gets
-// EUV_STATUS_TIMEOUT) or when another role already gave up.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
                                           int* err) {
-  const int r = bounded_spin([&] { return mbar_try(bar, parity); },
-                             [&] { return *abort_flag != 0; }, MX_TIMEOUT_NS);
-  if (r == 1) return true;
-  if (r < 0) {
-    *abort_flag = 1;
-    atomicOr(err, EUV_STATUS_TIMEOUT);
-  }
-  return false;
-}
-__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z,
-                                            uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
-      : "memory");
-}
-// K-major operand, 64-byte swizzle: 8-row atoms of 512 B (SBO), version 1.
-__device__ __forceinline__ uint64_t umma_desc_sw64(const void* tile) {
-  const uint64_t addr = smem_u32(tile);
-  uint64_t d = 0;
-  d |= (addr >> 4) & 0x3FFFull;          // start address
-  d |= (uint64_t)1 << 16;                // leading byte offset (unused for swizzled K-major)
-  d |= (uint64_t)(512 >> 4) << 32;       // stride byte offset: 8 rows x 64 B
-  d |= (uint64_t)1 << 46;                // descriptor version (sm_100)
-  d |= (uint64_t)4 << 61;                // SWIZZLE_64B
-  return d;
+  return mbar_wait_bounded(bar, parity, abort_flag, err, MX_TIMEOUT_NS);
 }
 __device__ __forceinline__ constexpr uint32_t idesc_tf32(bool neg_a) {
-  return (1u << 4)                       // D: F32
-         | (2u << 7) | (2u << 10)        // A, B: TF32
-         | ((neg_a ? 1u : 0u) << 13)     // negate A
-         | ((uint32_t)(MX_BN >> 3) << 17) // N
-         | ((uint32_t)(MX_BM >> 4) << 24);// M
-}
-__device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc,
-                                          uint32_t accumulate) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-      "l"(da), "l"(db), "r"(idesc), "r"(accumulate)
-      : "memory");
-}
-__device__ __forceinline__ void umma_commit(uint64_t* bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                   smem_u32(bar))
-               : "memory");
-}
-__device__ __forceinline__ void tc_fence_before() {
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-}
-__device__ __forceinline__ void tc_fence_after() {
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-}
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,"
-      "%15}, [%16];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-        "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
-}
-__device__ __forceinline__ void tmem_ld_wait() {
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+  return idesc_tf32_mn(neg_a, MX_BM, MX_BN);
 }
 
 __global__ void __launch_bounds__(MX_THREADS, 1)
@@ -355,14 +268,6 @@ __global__ void __launch_bounds__(MX_THREADS, 1)
   }
 }
 
-__device__ __forceinline__ void split_tf32(double x, float& hi, float& lo) {
-  const float f = (float)x;
-  uint32_t h;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(f));
-  hi = __uint_as_float(h);
-  lo = (float)(x - (double)hi);
-}
-
 // A (col-major complex M x K) -> planes [b][4][M][Kp], K contiguous (transpose
 // through a 32x32 shared tile).
 __global__ void split_a_kernel(int M, int K, int Kp, const double2* A, long long lda,
@@ -418,43 +323,12 @@ __global__ void split_b_kernel(int K, int N, int Kp, const double2* B, long long
 }
 
 // ------------------------------------------------------------------ host
-typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
-                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
-                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
-                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-static EncodeTiledFn encode_fn() {
-  static EncodeTiledFn fn = nullptr;
-  if (!fn) {
-    void* p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
-            cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<EncodeTiledFn>(p);
-  }
-  return fn;
-}
-
 // planes tensor [batch*4][rows][kp] fp32 -> 3-D map (kp, rows, batch*4), box (16, box_rows, 1)
 static int make_map(CUtensorMap* map, float* base, int rows, int kp, int nplanes, int box_rows) {
-  EncodeTiledFn enc = encode_fn();
-  if (!enc) {
-    euv_set_error("cuTensorMapEncodeTiled is not available from the driver");
-    return EUV_ERR_CUDA;
-  }
-  cuuint64_t dims[3] = {(cuuint64_t)kp, (cuuint64_t)rows, (cuuint64_t)nplanes};
-  cuuint64_t strides[2] = {(cuuint64_t)kp * 4, (cuuint64_t)kp * 4 * rows};
-  cuuint32_t box[3] = {(cuuint32_t)MX_BK, (cuuint32_t)box_rows, 1};
-  cuuint32_t estr[3] = {1, 1, 1};
-  CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, estr,
-                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
-                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) {
-    euv_set_error("cuTensorMapEncodeTiled failed (%d) rows=%d kp=%d", (int)r, rows, kp);
-    return EUV_ERR_CUDA;
-  }
-  return EUV_OK;
+  const cuuint64_t dims[3] = {(cuuint64_t)kp, (cuuint64_t)rows, (cuuint64_t)nplanes};
+  const cuuint64_t strides[2] = {(cuuint64_t)kp * 4, (cuuint64_t)kp * 4 * rows};
+  const cuuint32_t box[3] = {(cuuint32_t)MX_BK, (cuuint32_t)box_rows, 1};
+  return make_map_f32(map, base, 3, dims, strides, box);
 }
 
 static inline int round_up(int x, int a) { return (x + a - 1) / a * a; }

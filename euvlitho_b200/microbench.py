@@ -7,6 +7,7 @@
   python -m euvlitho_b200.microbench linear --preset reference --clips 1
   python -m euvlitho_b200.microbench raster --clips 64 --slices 8
   python -m euvlitho_b200.microbench socs   --preset reference --clips 4
+  python -m euvlitho_b200.microbench cnn    --clips 64
   python -m euvlitho_b200.microbench summarize launches.csv
 
 Times each library entry point with CUDA events on the launching stream after
@@ -23,6 +24,8 @@ Abbe images per clip) with tables resident, on seeded masks and parameters.
 2048^2 masks (layouts drawn on the host beforehand), with sidewall slices.
 `socs` times the STCC-SOCS tables (TCC GEMMs + three Jacobi eigensolves, once
 per configuration) and the per-clip SOCS images.
+`cnn` times the CNN predict (six networks, random weights) on --clips random
+mask rasters, tables resident.
 `summarize` folds an ncu `--csv` launch list of gpu__time_duration.sum into
 launches, total time and share per kernel.
 """
@@ -167,6 +170,60 @@ def _socs(a) -> dict:
             "tables_s": t_tab, "ms_per_call": ms, "clips_per_s": a.clips / (ms / 1e3)}
 
 
+def cnn_random_weights(n_outs, seed: int = 0):
+    """Random state_dicts of the CNN predict networks (default-init scales),
+    drawn on the device."""
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    ch = (1, 16, 32, 64, 128, 256)
+
+    def u(shape, fan_in):
+        b = 1.0 / fan_in ** 0.5
+        return (torch.rand(shape, generator=g, device="cuda") * 2 - 1) * b
+    sds = []
+    for n in n_outs:
+        sd = {}
+        for l in range(5):
+            sd["conv%d.weight" % (l + 1)] = u((ch[l + 1], ch[l], 3, 3), 9 * ch[l])
+            sd["conv%d.bias" % (l + 1)] = u((ch[l + 1],), 9 * ch[l])
+            c = ch[l + 1]
+            sd["norm%d.weight" % (l + 1)] = 1 + 0.2 * torch.randn(c, generator=g, device="cuda")
+            sd["norm%d.bias" % (l + 1)] = 0.2 * torch.randn(c, generator=g, device="cuda")
+            sd["norm%d.running_mean" % (l + 1)] = 0.2 * torch.randn(c, generator=g, device="cuda")
+            sd["norm%d.running_var" % (l + 1)] = 0.5 + torch.rand(c, generator=g, device="cuda")
+        sd["fc1.weight"] = u((4096, 65536), 65536)
+        sd["fc1.bias"] = u((4096,), 65536)
+        sd["fc2.weight"] = u((n, 4096), 4096)
+        sd["fc2.bias"] = u((n,), 4096)
+        sds.append(sd)
+    return sds
+
+
+# FP32-equivalent FLOP per mask and network: conv1..conv5 (2 x pixels x cout x
+# 9 cin) + fc1 + fc2
+def cnn_flop_per_mask(n_out: int) -> float:
+    conv = sum(2.0 * (512 >> l) ** 2 * (16 << l) * 9 * (1 if l == 0 else 8 << l) for l in range(5))
+    return conv + 2.0 * 65536 * 4096 + 2.0 * 4096 * n_out
+
+
+def _cnn(a) -> dict:
+    from . import cnn
+    n_outs = (1901, 1901, 1749, 1749, 1749, 1749)
+    pred = cnn.CnnPredictor(cnn_random_weights(n_outs),
+                            [torch.ones(n).numpy() for n in n_outs], torch.device("cuda"))
+    g = torch.Generator(device="cuda").manual_seed(1)
+    bits = torch.randint(0, 256, (a.clips, cnn.MASK_BYTES), generator=g, device="cuda",
+                         dtype=torch.uint8)
+    out = torch.empty((6, a.clips, pred.max_out), dtype=torch.float64, device="cuda")
+    ms = _time(lambda: pred.predict_device(bits, out), a.reps)
+    pred.check()
+    flop = a.clips * sum(cnn_flop_per_mask(n) for n in n_outs)
+    conv1 = a.clips * 6 * 2.0 * 512 ** 2 * 16 * 9
+    return {"masks": a.clips, "networks": 6, "ms_per_call": ms, "masks_per_s": a.clips / (ms / 1e3),
+            "fp32_equiv_tflops": flop / (ms / 1e3) / 1e12,
+            "tf32_tensor_tflops": 3 * (flop - conv1) / (ms / 1e3) / 1e12,
+            "fc1_weight_planes_gb": 6 * 2 * 4096 * 65536 * 4 / 1e9}
+
+
 def _time(fn, reps: int) -> float:
     for _ in range(3):
         fn()
@@ -185,7 +242,7 @@ def _time(fn, reps: int) -> float:
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("kernel", choices=["tf32x3", "zgemm", "lu", "step", "linear", "raster",
-                                       "socs", "summarize"])
+                                       "socs", "cnn", "summarize"])
     ap.add_argument("--slices", type=int, default=8)
     ap.add_argument("csv", nargs="?", help="ncu --csv launch list (summarize)")
     ap.add_argument("--n", type=int, default=961)
@@ -212,6 +269,9 @@ def main(argv=None) -> int:
         return 0
     if a.kernel == "socs":
         print(json.dumps(_socs(a)))
+        return 0
+    if a.kernel == "cnn":
+        print(json.dumps(_cnn(a)))
         return 0
     n, b = a.n, a.batch
     s = torch.cuda.current_stream().cuda_stream

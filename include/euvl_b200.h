@@ -168,6 +168,55 @@ int euv_mask_raster(int n_masks, int ndivx, int ndivy, int n_rects, const int* d
                     size_t work_bytes, void* stream);
 
 /* ------------------------------------------------------------------------ */
+/* CNN predict: replaces predict_m3d (cnn/cnn/predict/predict.py:108-121) with
+ * the networks CNNmodel / CNNmodels (predict.py:16-88) and the mask
+ * downsampling compmask (cnn/cnn/predict/compmask.py:17-41).
+ *
+ * A model is the reference's network: five [conv 3x3 circular, ReLU, 2x2
+ * max-pool, BatchNorm (running statistics)] stages 1-16-32-64-128-256 on a
+ * 512 x 512 input, fc1 65536 -> 4096 + ReLU, fc2 4096 -> n_out.  Weights are
+ * the torch tensors of a state_dict, fp32, contiguous, on the device, in torch
+ * layout (conv [cout][cin][3][3], linear [out][in]); euv_cnn_pack rewrites
+ * them once into a blob of TF32 (hi, lo) planes (about 2.2 GB per model).
+ * The predict takes mask.bin rasters (2048 x 2048 bits, MSB first, 524288
+ * bytes per mask), and writes out[model][mask][j] = fc2 output / factor
+ * (the division of predict.py:114-119, in double) for j < n_out[model],
+ * zero above.  Products are TF32x3 with FP32 accumulation (about FP32
+ * accuracy). */
+#define EUV_CNN_MAX_MODELS 6
+#define EUV_CNN_MAX_OUT 8192
+typedef struct euv_cnn_model_weights {
+  const float* conv_w[5]; /* conv1..conv5 weight, bias */
+  const float* conv_b[5];
+  const float* bn_w[5];   /* norm1..norm5 weight, bias, running_mean, running_var */
+  const float* bn_b[5];
+  const float* bn_mean[5];
+  const float* bn_var[5];
+  const float* fc1_w;     /* [4096][65536] */
+  const float* fc1_b;
+  const float* fc2_w;     /* [n_out][4096] */
+  const float* fc2_b;
+  int n_out;
+} euv_cnn_model_weights;
+
+typedef struct euv_cnn_desc {
+  int n_models, n_masks, max_out; /* max_out: row stride of d_factors and out */
+  int n_out[EUV_CNN_MAX_MODELS];
+  const double* d_factors;        /* [n_models][max_out] */
+  int* d_status;                  /* EUV_STATUS_* word, or NULL */
+} euv_cnn_desc;
+
+size_t euv_cnn_blob_bytes(int n_models, int max_out);
+int euv_cnn_pack(int n_models, const euv_cnn_model_weights* h_models, int max_out,
+                 double bn_eps, void* d_blob, size_t blob_bytes, void* stream);
+size_t euv_cnn_workspace_bytes(int n_models, int n_masks, int max_out);
+/* d_blob and d_work 256-byte aligned */
+int euv_cnn_predict(const euv_cnn_desc* desc, const uint8_t* d_bits, const void* d_blob,
+                    double* d_out, void* d_work, size_t work_bytes, void* stream);
+/* compmask alone: d_x0[mask][512][512] = 4 x 4 box means of the bits */
+int euv_cnn_downsample(int n_masks, const uint8_t* d_bits, float* d_x0, void* stream);
+
+/* ------------------------------------------------------------------------ */
 /* Batched ampS: replaces ampS (header.h:1208-1466) with multilayerS
  * (header.h:5-363), absorberS0 (754-1145), absorberS (365-752), matinv and
  * matproduct (1468-1619), for n_units independent problems that share one

@@ -61,6 +61,25 @@ def test_struct_sizes_match_c_layout():
     assert C.sizeof(L.Stack) == 6 * 16 + 6 * 8 + 8
 
 
+def test_cnn_entry_points_reject_bad_arguments(lib):
+    # validated before any launch or allocation: runs without a GPU
+    assert lib.euv_cnn_blob_bytes(0, 1901) == 0
+    assert lib.euv_cnn_blob_bytes(7, 1901) == 0
+    assert lib.euv_cnn_blob_bytes(6, L.EUV_CNN_MAX_OUT + 1) == 0
+    assert lib.euv_cnn_workspace_bytes(6, 0, 1901) == 0
+    # 6 networks: fc1 planes dominate (2 x 4096 x 65536 fp32 each)
+    assert lib.euv_cnn_blob_bytes(6, 1901) > 6 * 2 * 4096 * 65536 * 4
+    d = L.CnnDesc()
+    d.n_models, d.n_masks, d.max_out = 1, 1, 10
+    d.n_out[0] = 11  # above max_out
+    d.d_factors = 256
+    assert lib.euv_cnn_predict(C.byref(d), 1, 1, 1, 1, 1 << 30, None) == L.EUV_ERR_BAD_ARG
+    assert b"n_out" in lib.euv_last_error()
+    w = (L.CnnModelWeights * 1)()
+    assert lib.euv_cnn_pack(1, w, 10, 1e-5, 256, 1 << 40, None) == L.EUV_ERR_BAD_ARG
+    assert lib.euv_cnn_downsample(0, None, None, None) == L.EUV_ERR_BAD_ARG
+
+
 def test_wait_probe_rejects_bad_arguments(lib):
     # validated before any launch, so this runs without a GPU
     assert lib.euv_wait_probe(None, 1000, None, None) == L.EUV_ERR_BAD_ARG
@@ -73,7 +92,8 @@ def test_descriptor_layout_matches_the_header(tmp_path):
     ctypes mirrors."""
     import subprocess
     structs = {"euv_amp_desc": L.AmpDesc, "euv_abbe_desc": L.AbbeDesc, "euv_m3d_desc": L.M3dDesc,
-               "euv_stack": L.Stack, "euv_linear_desc": L.LinearDesc, "euv_socs_desc": L.SocsDesc}
+               "euv_stack": L.Stack, "euv_linear_desc": L.LinearDesc, "euv_socs_desc": L.SocsDesc,
+               "euv_cnn_desc": L.CnnDesc, "euv_cnn_model_weights": L.CnnModelWeights}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "euvl_b200.h"', "int main(void) {"]
     for cname, py in structs.items():
         lines.append('printf("%s size %%zu\\n", sizeof(%s));' % (cname, cname))
