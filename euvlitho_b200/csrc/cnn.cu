@@ -13,7 +13,7 @@
 //   cnn_input_kernel   bits -> 512^2 box means (popcount of 4x4 bit boxes / 16);
 //   cnn_conv1_kernel   conv1 (one input channel, 9 taps: CUDA cores, FP32) for all
 //                      models at once, fused bias/ReLU/pool/BN;
-//   cnn_gemm_kernel<CONV> conv2..conv5 as implicit GEMMs on tcgen05: M = 128
+//   cnn_conv_kernel    conv2..conv5 as persistent implicit GEMMs on tcgen05: M = 128
 //                      output pixels (an 8 x 16 block), N = output channels,
 //                      K = 9 taps x input channels.  Activations live as TF32
 //                      (hi, lo) planes in NHWC with a one-pixel circular halo,
@@ -22,7 +22,7 @@
 //                      takes the 2 x 2 pool maxima across lanes (shuffles),
 //                      adds bias, ReLU, BN, splits into (hi, lo) and writes the
 //                      next layer's padded planes including the halo copies;
-//   cnn_gemm_kernel<FC> fc1 and fc2 as split-K GEMMs (A = weight planes, N =
+//   cnn_fc_kernel      fc1 and fc2 as split-K GEMMs (A = weight planes, N =
 //                      masks), FP32 partial sums reduced by cnn_fc*_finish.
 // Products are TF32x3 (hi*hi + hi*lo + lo*hi, FP32 accumulation), about FP32
 // accuracy; split-K keeps each accumulator's K run short (the tensor-core FP32
@@ -263,52 +263,245 @@ __global__ void cnn_conv1_kernel(int B, const float* x0, const float* w, const f
 
 // ------------------------------------------------------------------ tcgen05 GEMM
 
-enum { CNN_CONV = 0, CNN_FC = 1 };
+// Shared-memory ring of a TF32x3 GEMM: per stage A (hi, lo) 128 x 16 fp32 and
+// B (hi, lo) bn x 16 fp32, 64-byte swizzled K-major.
+struct CnnRing {
+  uint8_t* base;
+  int stage_bytes, b_bytes;
+  __device__ uint8_t* a(int s, int pl) const { return base + s * stage_bytes + pl * CNN_A_TILE; }
+  __device__ uint8_t* b(int s, int pl) const {
+    return base + s * stage_bytes + 2 * CNN_A_TILE + pl * b_bytes;
+  }
+};
 
-struct CnnGemmArgs {
-  int models, batch;
-  int bn, nkb, stages;
-  // conv
-  int side, tiles_x, cin, cout, out_pad;
+// hi*hi + hi*lo + lo*hi of one 16-wide K block into the accumulator at tmem
+__device__ __forceinline__ void cnn_mma_block(const CnnRing& r, int s, uint32_t tmem,
+                                              uint32_t idesc, bool first) {
+#pragma unroll
+  for (int k8 = 0; k8 < CNN_BK / 8; ++k8) {
+    const uint64_t ah = umma_desc_sw64(r.a(s, 0) + k8 * 32);
+    const uint64_t al = umma_desc_sw64(r.a(s, 1) + k8 * 32);
+    const uint64_t bh = umma_desc_sw64(r.b(s, 0) + k8 * 32);
+    const uint64_t bl = umma_desc_sw64(r.b(s, 1) + k8 * 32);
+    umma_tf32(tmem, ah, bh, idesc, (first && k8 == 0) ? 0u : 1u);
+    umma_tf32(tmem, ah, bl, idesc, 1u);
+    umma_tf32(tmem, al, bh, idesc, 1u);
+  }
+}
+
+struct CnnConvArgs {
+  int models, batch, side, tiles_x, tiles_img, total_tiles;
+  int cin, cout, nkb, stages, out_pad;
   const float *bias, *scale, *shift;
   float* out;
-  // fc
+  int* err;
+};
+
+// Persistent implicit-GEMM convolution: a CTA walks the (model, mask, 8 x 16
+// pixel block) tiles blockIdx.x, + gridDim.x, ...  Warp 0 issues the TMA
+// loads of every tile's 9 taps x cin/16 K blocks into the stage ring, warp 1
+// the MMAs into one of two TMEM accumulators (tile parity), warps 2..5 the
+// epilogue of the previous tile meanwhile.  Barriers: full/empty per stage,
+// tfull (MMA -> epilogue) and tempty (epilogue, 4 warps -> MMA) per
+// accumulator.  All waits bounded; a timeout raises EUV_STATUS_TIMEOUT.
+__global__ void __launch_bounds__(CNN_THREADS) cnn_conv_kernel(
+    const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+    CnnConvArgs p) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  const int bn = p.cout;
+  CnnRing ring{smem, 2 * CNN_A_TILE + 2 * bn * CNN_BK * 4, bn * CNN_BK * 4};
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + p.stages * ring.stage_bytes);
+  uint64_t* empty = full + p.stages;
+  uint64_t* tfull = empty + p.stages;
+  uint64_t* tempty = tfull + 2;
+  uint64_t* done = tempty + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+  // epilogue constants of every model: bias | bn scale | bn shift, [models][cout] each
+  float* s_vec = reinterpret_cast<float*>(smem + p.stages * ring.stage_bytes + 256);
+  const int nvec = p.models * bn;
+  for (int i = threadIdx.x; i < nvec; i += blockDim.x) {
+    s_vec[i] = p.bias[i];
+    s_vec[nvec + i] = p.scale[i];
+    s_vec[2 * nvec + i] = p.shift[i];
+  }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint32_t tcols = 32;
+  while ((int)tcols < 2 * bn) tcols <<= 1;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < p.stages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(&tfull[i], 1);
+      mbar_init(&tempty[i], 4);
+    }
+    mbar_init(done, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == 1) tmem_alloc(tmem_slot, tcols);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const int cchunks = p.cin / CNN_BK;
+  // tile -> (model, img, y0, x0), model slowest so that concurrent CTAs share weights
+  auto decode = [&](int t, int& model, int& img, int& y0, int& x0) {
+    const int pt = t % p.tiles_img, mi = t / p.tiles_img;
+    img = mi % p.batch;
+    model = mi / p.batch;
+    y0 = 8 * (pt / p.tiles_x);
+    x0 = 16 * (pt % p.tiles_x);
+  };
+
+  if (warp == 0) {
+    if (lane == 0) {
+      int it = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; t < p.total_tiles && ok; t += gridDim.x) {
+        int model, img, y0, x0;
+        decode(t, model, img, y0, x0);
+        for (int kb = 0; kb < p.nkb; ++kb, ++it) {
+          const int s = it % p.stages;
+          if (!mbar_wait_bounded(&empty[s], (uint32_t)(((it / p.stages) & 1) ^ 1), abort_flag,
+                                 p.err, CNN_TIMEOUT_NS)) {
+            ok = false;
+            break;
+          }
+          mbar_expect_tx(&full[s], (uint32_t)ring.stage_bytes);
+          const int tap = kb / cchunks, cc = kb % cchunks;
+          const int ky = tap / 3, kx = tap % 3;
+          for (int pl = 0; pl < 2; ++pl)
+            tma_load_5d(ring.a(s, pl), &tmA, cc * CNN_BK, x0 + kx, y0 + ky, img, 2 * model + pl,
+                        &full[s]);
+          for (int pl = 0; pl < 2; ++pl)
+            tma_load_3d(ring.b(s, pl), &tmB, kb * CNN_BK, 0, 2 * model + pl, &full[s]);
+        }
+      }
+      if (!ok) {
+        for (int j = (it > p.stages ? it - p.stages : 0); j < it; ++j)
+          mbar_drain(&full[j % p.stages], (uint32_t)((j / p.stages) & 1), CNN_TIMEOUT_NS);
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      const uint32_t idesc = idesc_tf32_mn(false, 128, bn);
+      int it = 0, local = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; t < p.total_tiles && ok; t += gridDim.x, ++local) {
+        const int ab = local & 1;
+        if (!mbar_wait_bounded(&tempty[ab], (uint32_t)(((local >> 1) & 1) ^ 1), abort_flag,
+                               p.err, CNN_TIMEOUT_NS)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        for (int kb = 0; kb < p.nkb; ++kb, ++it) {
+          const int s = it % p.stages;
+          if (!mbar_wait_bounded(&full[s], (uint32_t)((it / p.stages) & 1), abort_flag, p.err,
+                                 CNN_TIMEOUT_NS)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          cnn_mma_block(ring, s, tmem + (uint32_t)(ab * bn), idesc, kb == 0);
+          umma_commit(&empty[s]);
+        }
+        if (ok) umma_commit(&tfull[ab]);
+      }
+      umma_commit(done);  // always: teardown after an abort waits for the MMAs in flight
+    }
+  } else {
+    const int q = warp & 3;
+    const uint32_t lane_addr = (uint32_t)(q * 32) << 16;
+    // TMEM lane = pixel h*16 + w of the 8 x 16 block: a warp holds rows 2q, 2q+1
+    const int h = 2 * q + (lane >> 4), w = lane & 15;
+    const bool owner = (lane & 17) == 0;
+    const int so = p.side / 2, pad = p.out_pad, hp = so + 2 * pad;
+    const long long img_elems = (long long)hp * hp * p.cout;
+    const long long plane = (long long)p.batch * img_elems;
+    int local = 0;
+    for (int t = blockIdx.x; t < p.total_tiles; t += gridDim.x, ++local) {
+      const int ab = local & 1;
+      const bool waited = mbar_wait_bounded(&tfull[ab], (uint32_t)((local >> 1) & 1), abort_flag,
+                                            p.err, CNN_TIMEOUT_NS) && !*abort_flag;
+      if (!__all_sync(0xffffffffu, waited)) break;
+      tc_fence_after();
+      int model, img, y0, x0;
+      decode(t, model, img, y0, x0);
+      const int py = (y0 + h) >> 1, px = (x0 + w) >> 1;
+      float* base = p.out + (long long)model * 2 * plane + (long long)img * img_elems;
+      const float* bias = s_vec + model * bn;
+      const float* scale = bias + nvec;
+      const float* shift = scale + nvec;
+      for (int c0 = 0; c0 < p.cout; c0 += 16) {
+        uint32_t v[16];
+        tmem_ld16(tmem + lane_addr + (uint32_t)(ab * bn + c0), v);
+        tmem_ld_wait();
+        float hi[16], lo[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          float f = __uint_as_float(v[j]);
+          f = fmaxf(f, __shfl_xor_sync(0xffffffffu, f, 1));
+          f = fmaxf(f, __shfl_xor_sync(0xffffffffu, f, 16));
+          const int c = c0 + j;
+          const float y = fmaxf(f + bias[c], 0.0f) * scale[c] + shift[c];
+          split_tf32f(y, hi[j], lo[j]);
+        }
+        if (owner) cnn_store16(base, plane, so, pad, p.cout, py, px, c0, hi, lo);
+      }
+      // this warp's TMEM reads are complete: hand the accumulator back
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0)
+        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&tempty[ab]))
+                     : "memory");
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    // the MMAs in flight (after an abort) and the final commit's arrival
+    mbar_drain(done, 0u, CNN_TIMEOUT_NS);
+    tmem_dealloc(tmem, tcols);
+  }
+}
+
+struct CnnFcArgs {
+  int models, batch;
+  int bn, nkb, stages;
   int rows, nsplit;
   float* part;
   int* err;
 };
 
-template <int MODE>
-__global__ void __launch_bounds__(CNN_THREADS) cnn_gemm_kernel(
+// Split-K fully connected layer: A = weight planes [2M][rows][K] (128 rows per
+// CTA), B = activation planes [2M][batch][K] (bn masks per CTA), K range
+// split blockIdx.y % nsplit; FP32 partial sums to part[split][model][mask][row].
+__global__ void __launch_bounds__(CNN_THREADS) cnn_fc_kernel(
     const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-    CnnGemmArgs p) {
+    CnnFcArgs p) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
-  const int b_tile_bytes = p.bn * CNN_BK * 4;
-  const int stage_bytes = 2 * CNN_A_TILE + 2 * b_tile_bytes;
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem + p.stages * stage_bytes);
+  CnnRing ring{smem, 2 * CNN_A_TILE + 2 * p.bn * CNN_BK * 4, p.bn * CNN_BK * 4};
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + p.stages * ring.stage_bytes);
   uint64_t* empty = full + p.stages;
   uint64_t* accum = empty + p.stages;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accum + 1);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
-  auto a_tile = [&](int s, int pl) { return smem + s * stage_bytes + pl * CNN_A_TILE; };
-  auto b_tile = [&](int s, int pl) {
-    return smem + s * stage_bytes + 2 * CNN_A_TILE + pl * b_tile_bytes;
-  };
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int model = blockIdx.z;
-  // CTA coordinates
-  int img = 0, y0 = 0, x0 = 0, m0 = 0, n0 = 0, split = 0;
-  if (MODE == CNN_CONV) {
-    img = blockIdx.y;
-    y0 = 8 * (blockIdx.x / p.tiles_x);
-    x0 = 16 * (blockIdx.x % p.tiles_x);
-  } else {
-    m0 = 128 * blockIdx.x;
-    split = blockIdx.y % p.nsplit;
-    n0 = p.bn * (blockIdx.y / p.nsplit);
-  }
+  const int m0 = 128 * blockIdx.x;
+  const int split = blockIdx.y % p.nsplit;
+  const int n0 = p.bn * (blockIdx.y / p.nsplit);
   uint32_t tcols = 32;
   while ((int)tcols < p.bn) tcols <<= 1;
 
@@ -332,27 +525,16 @@ __global__ void __launch_bounds__(CNN_THREADS) cnn_gemm_kernel(
   if (warp == 0) {
     if (lane == 0) {
       int issued = 0;
-      const int cchunks = p.cin / CNN_BK;
       for (int kb = 0; kb < nkb; ++kb) {
         const int s = kb % p.stages;
         const uint32_t ph = (uint32_t)((kb / p.stages) & 1);
         if (!mbar_wait_bounded(&empty[s], ph ^ 1u, abort_flag, p.err, CNN_TIMEOUT_NS)) break;
-        mbar_expect_tx(&full[s], (uint32_t)stage_bytes);
-        if (MODE == CNN_CONV) {
-          const int tap = kb / cchunks, cc = kb % cchunks;
-          const int ky = tap / 3, kx = tap % 3;
-          for (int pl = 0; pl < 2; ++pl)
-            tma_load_5d(a_tile(s, pl), &tmA, cc * CNN_BK, x0 + kx, y0 + ky, img, 2 * model + pl,
-                        &full[s]);
-          for (int pl = 0; pl < 2; ++pl)
-            tma_load_3d(b_tile(s, pl), &tmB, kb * CNN_BK, 0, 2 * model + pl, &full[s]);
-        } else {
-          const int k0 = (split * nkb + kb) * CNN_BK;
-          for (int pl = 0; pl < 2; ++pl)
-            tma_load_3d(a_tile(s, pl), &tmA, k0, m0, 2 * model + pl, &full[s]);
-          for (int pl = 0; pl < 2; ++pl)
-            tma_load_3d(b_tile(s, pl), &tmB, k0, n0, 2 * model + pl, &full[s]);
-        }
+        mbar_expect_tx(&full[s], (uint32_t)ring.stage_bytes);
+        const int k0 = (split * nkb + kb) * CNN_BK;
+        for (int pl = 0; pl < 2; ++pl)
+          tma_load_3d(ring.a(s, pl), &tmA, k0, m0, 2 * model + pl, &full[s]);
+        for (int pl = 0; pl < 2; ++pl)
+          tma_load_3d(ring.b(s, pl), &tmB, k0, n0, 2 * model + pl, &full[s]);
         issued = kb + 1;
       }
       if (*abort_flag) {
@@ -368,16 +550,7 @@ __global__ void __launch_bounds__(CNN_THREADS) cnn_gemm_kernel(
         const uint32_t ph = (uint32_t)((kb / p.stages) & 1);
         if (!mbar_wait_bounded(&full[s], ph, abort_flag, p.err, CNN_TIMEOUT_NS)) break;
         tc_fence_after();
-#pragma unroll
-        for (int k8 = 0; k8 < CNN_BK / 8; ++k8) {
-          const uint64_t ah = umma_desc_sw64(a_tile(s, 0) + k8 * 32);
-          const uint64_t al = umma_desc_sw64(a_tile(s, 1) + k8 * 32);
-          const uint64_t bh = umma_desc_sw64(b_tile(s, 0) + k8 * 32);
-          const uint64_t bl = umma_desc_sw64(b_tile(s, 1) + k8 * 32);
-          umma_tf32(tmem, ah, bh, idesc, (kb | k8) ? 1u : 0u);
-          umma_tf32(tmem, ah, bl, idesc, 1u);
-          umma_tf32(tmem, al, bh, idesc, 1u);
-        }
+        cnn_mma_block(ring, s, tmem, idesc, kb == 0);
         umma_commit(&empty[s]);
       }
       umma_commit(accum);
@@ -389,36 +562,7 @@ __global__ void __launch_bounds__(CNN_THREADS) cnn_gemm_kernel(
     const bool ok = __all_sync(0xffffffffu, waited);
     tc_fence_after();
     const uint32_t lane_addr = (uint32_t)(q * 32) << 16;
-    if (ok && MODE == CNN_CONV) {
-      // TMEM lane = pixel h*16 + w of the 8 x 16 block: a warp holds rows 2q, 2q+1
-      const int h = 2 * q + (lane >> 4), w = lane & 15;
-      const bool owner = (lane & 17) == 0;
-      const int so = p.side / 2, pad = p.out_pad;
-      const int py = (y0 + h) >> 1, px = (x0 + w) >> 1;
-      const int hp = so + 2 * pad;
-      const long long img_elems = (long long)hp * hp * p.cout;
-      const long long plane = (long long)p.batch * img_elems;
-      float* base = p.out + (long long)model * 2 * plane + (long long)img * img_elems;
-      const float* bias = p.bias + model * p.cout;
-      const float* scale = p.scale + model * p.cout;
-      const float* shift = p.shift + model * p.cout;
-      for (int c0 = 0; c0 < p.cout; c0 += 16) {
-        uint32_t v[16];
-        tmem_ld16(tmem + lane_addr + (uint32_t)c0, v);
-        tmem_ld_wait();
-        float hi[16], lo[16];
-#pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          float f = __uint_as_float(v[j]);
-          f = fmaxf(f, __shfl_xor_sync(0xffffffffu, f, 1));
-          f = fmaxf(f, __shfl_xor_sync(0xffffffffu, f, 16));
-          const int c = c0 + j;
-          const float y = fmaxf(f + bias[c], 0.0f) * scale[c] + shift[c];
-          split_tf32f(y, hi[j], lo[j]);
-        }
-        if (owner) cnn_store16(base, plane, so, pad, p.cout, py, px, c0, hi, lo);
-      }
-    } else if (ok) {
+    if (ok) {
       const int row = m0 + q * 32 + lane;
       float* part = p.part + ((long long)split * p.models + model) * p.batch * p.rows;
       for (int c0 = 0; c0 < p.bn; c0 += 16) {
@@ -499,21 +643,51 @@ static size_t cnn_smem(int bn, int stages) {
   return (size_t)stages * (2 * CNN_A_TILE + 2 * bn * CNN_BK * 4) + 1024 + 256;
 }
 
-template <int MODE>
-static int cnn_launch(dim3 grid, const CUtensorMap& ta, const CUtensorMap& tb,
-                      const CnnGemmArgs& p, cudaStream_t stream) {
-  const size_t smem = cnn_smem(p.bn, p.stages);
-  static int done[64];
+template <class Kern, class Args>
+static int cnn_launch(Kern kernel, dim3 grid, size_t smem, const CUtensorMap& ta,
+                      const CUtensorMap& tb, const Args& p, cudaStream_t stream, int* done) {
   int dev = 0;
   EUV_CUDA_TRY(cudaGetDevice(&dev));
   if (dev < 64 && done[dev] < (int)smem) {
-    EUV_CUDA_TRY(cudaFuncSetAttribute(cnn_gemm_kernel<MODE>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    EUV_CUDA_TRY(
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     done[dev] = (int)smem;
   }
-  cnn_gemm_kernel<MODE><<<grid, CNN_THREADS, smem, stream>>>(ta, tb, p);
+  kernel<<<grid, CNN_THREADS, smem, stream>>>(ta, tb, p);
   EUV_LAUNCH_CHECK();
   return EUV_OK;
+}
+
+// persistent grid of the conv kernel: resident CTAs per SM by shared memory
+// (with the 1 KB the runtime reserves per CTA) and registers, capped by TMEM
+// (two accumulators of cout columns each, allocated as a power of two)
+static int cnn_conv_grid(int total, int cout, size_t smem) {
+  static int done[64];
+  int dev = 0, nsm = 148, sm_smem = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return -1;
+  if (dev < 64 && done[dev] < (int)smem) {
+    if (cudaFuncSetAttribute(cnn_conv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess ||
+        cudaFuncSetAttribute(cnn_conv_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             (int)cudaSharedmemCarveoutMaxShared) != cudaSuccess)
+      return -1;
+    done[dev] = (int)smem;
+  }
+  cudaFuncAttributes fa;
+  if (cudaFuncGetAttributes(&fa, cnn_conv_kernel) != cudaSuccess ||
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sm_smem, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) !=
+          cudaSuccess)
+    return -1;
+  int occ = sm_smem / (int)(smem + 1024 + fa.sharedSizeBytes);
+  const int regs = ((fa.numRegs + 7) / 8) * 8 * CNN_THREADS;
+  if (regs > 0 && occ > 65536 / regs) occ = 65536 / regs;
+  int tcols = 32;
+  while (tcols < 2 * cout) tcols <<= 1;
+  if (occ > 512 / tcols) occ = 512 / tcols;
+  if (occ < 1) occ = 1;
+  const long long g = (long long)nsm * occ;
+  return (int)(g < total ? g : total);
 }
 
 }  // namespace euv
@@ -666,24 +840,36 @@ extern "C" int euv_cnn_predict(const euv_cnn_desc* d, const uint8_t* d_bits, con
     const cuuint32_t bbox[3] = {CNN_BK, (cuuint32_t)co, 1};
     rc = make_map_f32(&tb, const_cast<float*>(blob + L.w[l]), 3, bdims, bstr, bbox);
     if (rc) return rc;
-    CnnGemmArgs p = {};
-    p.models = M;
+    CnnConvArgs p = {};
     p.batch = B;
-    p.bn = co;
-    p.nkb = 9 * ci / CNN_BK;
-    p.stages = cnn_stages(co);
     p.side = S;
     p.tiles_x = S / 16;
+    p.tiles_img = (S / 8) * (S / 16);
+    const long long total = (long long)M * B * p.tiles_img;
+    if (total > 0x7fffffffLL) {
+      euv_set_error("euv_cnn_predict: too many conv tiles (%lld)", total);
+      return EUV_ERR_BAD_ARG;
+    }
+    p.total_tiles = (int)total;
+    p.models = M;
     p.cin = ci;
     p.cout = co;
+    p.nkb = 9 * ci / CNN_BK;
+    p.stages = cnn_stages(co);
     p.out_pad = l < 4 ? 1 : 0;
     p.bias = blob + L.bias[l];
     p.scale = blob + L.scale[l];
     p.shift = blob + L.shift[l];
     p.out = work + W.act[l];
     p.err = err;
-    dim3 grid((S / 8) * (S / 16), B, M);
-    if ((rc = cnn_launch<CNN_CONV>(grid, ta, tb, p, stream))) return rc;
+    const size_t smem = cnn_smem(co, p.stages) + (size_t)12 * M * co;
+    const int grid = cnn_conv_grid(p.total_tiles, co, smem);
+    if (grid < 1) {
+      euv_set_error("euv_cnn_predict: conv kernel setup failed");
+      return EUV_ERR_CUDA;
+    }
+    cnn_conv_kernel<<<grid, CNN_THREADS, smem, stream>>>(ta, tb, p);
+    EUV_LAUNCH_CHECK();
   }
   // fc1, fc2: A = weight planes [M*2][rows][K], B = activation planes [M*2][B][K]
   const int bn = B >= 256 ? 256 : (B + 15) / 16 * 16;
@@ -705,7 +891,7 @@ extern "C" int euv_cnn_predict(const euv_cnn_desc* d, const uint8_t* d_bits, con
     const cuuint32_t bbox[3] = {CNN_BK, (cuuint32_t)bn, 1};
     rc = make_map_f32(&tb, act, 3, bdims, bstr, bbox);
     if (rc) return rc;
-    CnnGemmArgs p = {};
+    CnnFcArgs p = {};
     p.models = M;
     p.batch = B;
     p.bn = bn;
@@ -716,7 +902,10 @@ extern "C" int euv_cnn_predict(const euv_cnn_desc* d, const uint8_t* d_bits, con
     p.part = work + (f == 0 ? W.part1 : W.part2);
     p.err = err;
     dim3 grid(rows / 128, ntiles * nsplit, M);
-    if ((rc = cnn_launch<CNN_FC>(grid, ta, tb, p, stream))) return rc;
+    static int fc_done[64];
+    if ((rc = cnn_launch(cnn_fc_kernel, grid, cnn_smem(bn, p.stages), ta, tb, p, stream,
+                         fc_done)))
+      return rc;
     if (f == 0) {
       const long long n = (long long)M * B * CNN_FC1_N;
       cnn_fc1_finish_kernel<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(

@@ -207,21 +207,23 @@ def cnn_flop_per_mask(n_out: int) -> float:
 
 def _cnn(a) -> dict:
     from . import cnn
-    n_outs = (1901, 1901, 1749, 1749, 1749, 1749)
+    n_outs = (1901, 1901, 1749, 1749, 1749, 1749)[:a.networks]
     pred = cnn.CnnPredictor(cnn_random_weights(n_outs),
                             [torch.ones(n).numpy() for n in n_outs], torch.device("cuda"))
+    torch.cuda.empty_cache()  # the fp32 weights are packed: release them
     g = torch.Generator(device="cuda").manual_seed(1)
     bits = torch.randint(0, 256, (a.clips, cnn.MASK_BYTES), generator=g, device="cuda",
                          dtype=torch.uint8)
-    out = torch.empty((6, a.clips, pred.max_out), dtype=torch.float64, device="cuda")
+    out = torch.empty((len(n_outs), a.clips, pred.max_out), dtype=torch.float64, device="cuda")
     ms = _time(lambda: pred.predict_device(bits, out), a.reps)
     pred.check()
     flop = a.clips * sum(cnn_flop_per_mask(n) for n in n_outs)
-    conv1 = a.clips * 6 * 2.0 * 512 ** 2 * 16 * 9
-    return {"masks": a.clips, "networks": 6, "ms_per_call": ms, "masks_per_s": a.clips / (ms / 1e3),
+    conv1 = a.clips * len(n_outs) * 2.0 * 512 ** 2 * 16 * 9
+    return {"masks": a.clips, "networks": len(n_outs), "ms_per_call": ms,
+            "masks_per_s": a.clips / (ms / 1e3),
             "fp32_equiv_tflops": flop / (ms / 1e3) / 1e12,
             "tf32_tensor_tflops": 3 * (flop - conv1) / (ms / 1e3) / 1e12,
-            "fc1_weight_planes_gb": 6 * 2 * 4096 * 65536 * 4 / 1e9}
+            "fc1_weight_planes_gb": len(n_outs) * 2 * 4096 * 65536 * 4 / 1e9}
 
 
 def _time(fn, reps: int) -> float:
@@ -252,6 +254,7 @@ def main(argv=None) -> int:
     ap.add_argument("--preset", default="batched")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--clips", type=int, default=4)
+    ap.add_argument("--networks", type=int, default=6, help="cnn: networks (1..6)")
     ap.add_argument("--compare", action="store_true",
                     help="step: also run the FP64 form and report the intensity error")
     a = ap.parse_args(argv)
