@@ -52,8 +52,10 @@ static inline size_t al256(size_t n) { return (n + 255) / 256 * 256; }  // in fl
 // Packed weights (floats, sections 1 KB aligned), every section [model]-major:
 //   conv1 w [M][16][9]; per layer l: (l >= 1) w planes [M][2][cout][9 cin] with
 //   K = (ky*3 + kx)*cin + c, then bias, bn scale, bn shift [M][cout];
-//   fc1 planes [M][2][4096][65536] (K in (h, w, c) order), bias [M][4096];
-//   fc2 planes [M][2][OP][4096] (rows >= n_out zero), bias [M][OP].
+//   fc1 w [M][4096][65536] fp32 (K in (h, w, c) order), bias [M][4096];
+//   fc2 w [M][OP][4096] fp32 (rows >= n_out zero), bias [M][OP].
+// The fc weights stay fp32 (the fc kernel splits them in shared memory: half
+// the HBM stream of stored planes); the conv weights are stored as planes.
 struct CnnBlob {
   size_t w[5], bias[5], scale[5], shift[5];
   size_t fc1, fc1_b, fc2, fc2_b, total;
@@ -74,11 +76,11 @@ static CnnBlob cnn_blob(int M, int max_out) {
     o += al256((size_t)M * cnn_cout(l));
   }
   b.fc1 = o;
-  o += al256((size_t)M * 2 * CNN_FC1_N * CNN_FC1_K);
+  o += al256((size_t)M * CNN_FC1_N * CNN_FC1_K);
   b.fc1_b = o;
   o += al256((size_t)M * CNN_FC1_N);
   b.fc2 = o;
-  o += al256((size_t)M * 2 * b.op * CNN_FC1_N);
+  o += al256((size_t)M * b.op * CNN_FC1_N);
   b.fc2_b = o;
   o += al256((size_t)M * b.op);
   b.total = o;
@@ -131,8 +133,8 @@ __global__ void cnn_pack_conv_kernel(int cout, int cin, const float* w, float* d
   dst[(long long)cout * kk + t] = lo;
 }
 
-// torch [rows][K] -> planes [2][rows_pad][K]; perm: K from (c, h, w) of a
-// 256 x 16 x 16 map to (h, w, c)
+// torch [rows][K] -> fp32 [rows_pad][K] (rows >= rows zero); perm: K from
+// (c, h, w) of a 256 x 16 x 16 map to (h, w, c)
 __global__ void cnn_pack_fc_kernel(int rows, int rows_pad, int K, int perm, const float* w,
                                    float* dst) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -144,10 +146,7 @@ __global__ void cnn_pack_fc_kernel(int rows, int rows_pad, int K, int perm, cons
     const int ko = perm ? (kn % 256) * 256 + kn / 256 : kn;
     v = w[(long long)r * K + ko];
   }
-  float hi, lo;
-  split_tf32f(v, hi, lo);
-  dst[t] = hi;
-  dst[n + t] = lo;
+  dst[t] = v;
 }
 
 // bias (zero beyond n), BN eval as scale = gamma / sqrt(var + eps),
@@ -291,36 +290,50 @@ __device__ __forceinline__ void cnn_mma_block(const CnnRing& r, int s, uint32_t 
 
 struct CnnConvArgs {
   int models, batch, side, tiles_x, tiles_img, total_tiles;
-  int cin, cout, nkb, stages, out_pad;
+  int cin, cout, mt, nbuf, a_stages, b_stages, out_pad;
   const float *bias, *scale, *shift;
   float* out;
   int* err;
 };
 
-// Persistent implicit-GEMM convolution: a CTA walks the (model, mask, 8 x 16
-// pixel block) tiles blockIdx.x, + gridDim.x, ...  Warp 0 issues the TMA
-// loads of every tile's 9 taps x cin/16 K blocks into the stage ring, warp 1
-// the MMAs into one of two TMEM accumulators (tile parity), warps 2..5 the
-// epilogue of the previous tile meanwhile.  Barriers: full/empty per stage,
-// tfull (MMA -> epilogue) and tempty (epilogue, 4 warps -> MMA) per
-// accumulator.  All waits bounded; a timeout raises EUV_STATUS_TIMEOUT.
+// bytes of one A plane of a conv stage: the (8 mt + 2) x 16 pixel halo block
+// of 16 channels (64 B rows)
+__host__ __device__ constexpr int cnn_conv_a_plane(int mt) { return (8 * mt + 2) * 16 * 64; }
+
+// Persistent implicit-GEMM convolution.  A CTA tile is mt blocks of 8 x 16
+// output pixels stacked in y (M = 128 pixels each, one TMEM accumulator of
+// cout columns each), walked as blockIdx.x, + gridDim.x, ... over (model,
+// mask, tile).  Per tile and per (kx, 16-channel chunk) warp 0 loads one
+// (8 mt + 2) x 16 halo block of the padded input planes (hi, lo) at x offset
+// kx; the three ky taps are that block shifted by ky rows of 16 pixels (a
+// 1 KB descriptor offset, a whole number of 64-byte swizzle atoms), each with
+// its own weight tile (hi, lo) from a second ring.  Warp 1 issues the TF32x3
+// MMAs of all mt blocks against each weight tile; warps 2..5 run the fused
+// epilogue of the previous tile meanwhile (nbuf = 2 accumulator sets when
+// TMEM holds them).  Barriers: full/empty per A and per B stage, tfull (MMA ->
+// epilogue) and tempty (epilogue, 4 warps -> MMA) per accumulator set.  All
+// waits bounded; a timeout raises EUV_STATUS_TIMEOUT.
 __global__ void __launch_bounds__(CNN_THREADS) cnn_conv_kernel(
     const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
     CnnConvArgs p) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
-  const int bn = p.cout;
-  CnnRing ring{smem, 2 * CNN_A_TILE + 2 * bn * CNN_BK * 4, bn * CNN_BK * 4};
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem + p.stages * ring.stage_bytes);
-  uint64_t* empty = full + p.stages;
-  uint64_t* tfull = empty + p.stages;
+  const int bn = p.cout, mt = p.mt;
+  const int a_plane = cnn_conv_a_plane(mt), b_plane = bn * CNN_BK * 4;
+  uint8_t* a_ring = smem;
+  uint8_t* b_ring = smem + p.a_stages * 2 * a_plane;
+  uint64_t* afull = reinterpret_cast<uint64_t*>(b_ring + p.b_stages * 2 * b_plane);
+  uint64_t* aempty = afull + p.a_stages;
+  uint64_t* bfull = aempty + p.a_stages;
+  uint64_t* bempty = bfull + p.b_stages;
+  uint64_t* tfull = bempty + p.b_stages;
   uint64_t* tempty = tfull + 2;
   uint64_t* done = tempty + 2;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
   // epilogue constants of every model: bias | bn scale | bn shift, [models][cout] each
-  float* s_vec = reinterpret_cast<float*>(smem + p.stages * ring.stage_bytes + 256);
+  float* s_vec = reinterpret_cast<float*>(reinterpret_cast<uint8_t*>(afull) + 512);
   const int nvec = p.models * bn;
   for (int i = threadIdx.x; i < nvec; i += blockDim.x) {
     s_vec[i] = p.bias[i];
@@ -329,12 +342,16 @@ __global__ void __launch_bounds__(CNN_THREADS) cnn_conv_kernel(
   }
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   uint32_t tcols = 32;
-  while ((int)tcols < 2 * bn) tcols <<= 1;
+  while ((int)tcols < p.nbuf * mt * bn) tcols <<= 1;
 
   if (threadIdx.x == 0) {
-    for (int s = 0; s < p.stages; ++s) {
-      mbar_init(&full[s], 1);
-      mbar_init(&empty[s], 1);
+    for (int s = 0; s < p.a_stages; ++s) {
+      mbar_init(&afull[s], 1);
+      mbar_init(&aempty[s], 1);
+    }
+    for (int s = 0; s < p.b_stages; ++s) {
+      mbar_init(&bfull[s], 1);
+      mbar_init(&bempty[s], 1);
     }
     for (int i = 0; i < 2; ++i) {
       mbar_init(&tfull[i], 1);
@@ -356,71 +373,113 @@ __global__ void __launch_bounds__(CNN_THREADS) cnn_conv_kernel(
     const int pt = t % p.tiles_img, mi = t / p.tiles_img;
     img = mi % p.batch;
     model = mi / p.batch;
-    y0 = 8 * (pt / p.tiles_x);
+    y0 = 8 * mt * (pt / p.tiles_x);
     x0 = 16 * (pt % p.tiles_x);
   };
 
   if (warp == 0) {
     if (lane == 0) {
-      int it = 0;
+      int ia = 0, ib = 0;
       bool ok = true;
       for (int t = blockIdx.x; t < p.total_tiles && ok; t += gridDim.x) {
         int model, img, y0, x0;
         decode(t, model, img, y0, x0);
-        for (int kb = 0; kb < p.nkb; ++kb, ++it) {
-          const int s = it % p.stages;
-          if (!mbar_wait_bounded(&empty[s], (uint32_t)(((it / p.stages) & 1) ^ 1), abort_flag,
-                                 p.err, CNN_TIMEOUT_NS)) {
-            ok = false;
-            break;
+        for (int kx = 0; kx < 3 && ok; ++kx)
+          for (int cc = 0; cc < cchunks && ok; ++cc, ++ia) {
+            const int sa = ia % p.a_stages;
+            if (!mbar_wait_bounded(&aempty[sa], (uint32_t)(((ia / p.a_stages) & 1) ^ 1),
+                                   abort_flag, p.err, CNN_TIMEOUT_NS)) {
+              ok = false;
+              break;
+            }
+            mbar_expect_tx(&afull[sa], (uint32_t)(2 * a_plane));
+            for (int pl = 0; pl < 2; ++pl)
+              tma_load_5d(a_ring + (sa * 2 + pl) * a_plane, &tmA, cc * CNN_BK, x0 + kx, y0, img,
+                          2 * model + pl, &afull[sa]);
+            for (int ky = 0; ky < 3; ++ky, ++ib) {
+              const int sb = ib % p.b_stages;
+              if (!mbar_wait_bounded(&bempty[sb], (uint32_t)(((ib / p.b_stages) & 1) ^ 1),
+                                     abort_flag, p.err, CNN_TIMEOUT_NS)) {
+                ok = false;
+                break;
+              }
+              mbar_expect_tx(&bfull[sb], (uint32_t)(2 * b_plane));
+              const int k0 = (3 * ky + kx) * p.cin + cc * CNN_BK;
+              for (int pl = 0; pl < 2; ++pl)
+                tma_load_3d(b_ring + (sb * 2 + pl) * b_plane, &tmB, k0, 0, 2 * model + pl,
+                            &bfull[sb]);
+            }
           }
-          mbar_expect_tx(&full[s], (uint32_t)ring.stage_bytes);
-          const int tap = kb / cchunks, cc = kb % cchunks;
-          const int ky = tap / 3, kx = tap % 3;
-          for (int pl = 0; pl < 2; ++pl)
-            tma_load_5d(ring.a(s, pl), &tmA, cc * CNN_BK, x0 + kx, y0 + ky, img, 2 * model + pl,
-                        &full[s]);
-          for (int pl = 0; pl < 2; ++pl)
-            tma_load_3d(ring.b(s, pl), &tmB, kb * CNN_BK, 0, 2 * model + pl, &full[s]);
-        }
       }
       if (!ok) {
-        for (int j = (it > p.stages ? it - p.stages : 0); j < it; ++j)
-          mbar_drain(&full[j % p.stages], (uint32_t)((j / p.stages) & 1), CNN_TIMEOUT_NS);
+        // drain this thread's copies in flight (bounded) before the CTA exits
+        for (int j = (ia > p.a_stages ? ia - p.a_stages : 0); j < ia; ++j)
+          mbar_drain(&afull[j % p.a_stages], (uint32_t)((j / p.a_stages) & 1), CNN_TIMEOUT_NS);
+        for (int j = (ib > p.b_stages ? ib - p.b_stages : 0); j < ib; ++j)
+          mbar_drain(&bfull[j % p.b_stages], (uint32_t)((j / p.b_stages) & 1), CNN_TIMEOUT_NS);
       }
     }
   } else if (warp == 1) {
     if (lane == 0) {
       const uint32_t idesc = idesc_tf32_mn(false, 128, bn);
-      int it = 0, local = 0;
+      int ia = 0, ib = 0, local = 0;
       bool ok = true;
       for (int t = blockIdx.x; t < p.total_tiles && ok; t += gridDim.x, ++local) {
-        const int ab = local & 1;
-        if (!mbar_wait_bounded(&tempty[ab], (uint32_t)(((local >> 1) & 1) ^ 1), abort_flag,
-                               p.err, CNN_TIMEOUT_NS)) {
+        const int ab = local % p.nbuf, use = local / p.nbuf;
+        if (!mbar_wait_bounded(&tempty[ab], (uint32_t)((use & 1) ^ 1), abort_flag, p.err,
+                               CNN_TIMEOUT_NS)) {
           ok = false;
           break;
         }
         tc_fence_after();
-        for (int kb = 0; kb < p.nkb; ++kb, ++it) {
-          const int s = it % p.stages;
-          if (!mbar_wait_bounded(&full[s], (uint32_t)((it / p.stages) & 1), abort_flag, p.err,
-                                 CNN_TIMEOUT_NS)) {
-            ok = false;
-            break;
+        const uint32_t acc = tmem + (uint32_t)(ab * mt * bn);
+        for (int kx = 0; kx < 3 && ok; ++kx)
+          for (int cc = 0; cc < cchunks && ok; ++cc, ++ia) {
+            const int sa = ia % p.a_stages;
+            if (!mbar_wait_bounded(&afull[sa], (uint32_t)((ia / p.a_stages) & 1), abort_flag,
+                                   p.err, CNN_TIMEOUT_NS)) {
+              ok = false;
+              break;
+            }
+            for (int ky = 0; ky < 3; ++ky, ++ib) {
+              const int sb = ib % p.b_stages;
+              if (!mbar_wait_bounded(&bfull[sb], (uint32_t)((ib / p.b_stages) & 1), abort_flag,
+                                     p.err, CNN_TIMEOUT_NS)) {
+                ok = false;
+                break;
+              }
+              tc_fence_after();
+              const bool first = kx == 0 && cc == 0 && ky == 0;
+              const uint8_t* bh = b_ring + (sb * 2) * b_plane;
+              const uint8_t* bl = bh + b_plane;
+              for (int m = 0; m < mt; ++m) {
+                // rows (8 m + ky) * 16 .. + 127 of the halo block
+                const uint8_t* ah = a_ring + (sa * 2) * a_plane + (8 * m + ky) * 16 * 64;
+                const uint8_t* al = ah + a_plane;
+                const uint32_t d = acc + (uint32_t)(m * bn);
+#pragma unroll
+                for (int k8 = 0; k8 < CNN_BK / 8; ++k8) {
+                  const uint64_t dah = umma_desc_sw64(ah + k8 * 32);
+                  const uint64_t dal = umma_desc_sw64(al + k8 * 32);
+                  const uint64_t dbh = umma_desc_sw64(bh + k8 * 32);
+                  const uint64_t dbl = umma_desc_sw64(bl + k8 * 32);
+                  umma_tf32(d, dah, dbh, idesc, (first && k8 == 0) ? 0u : 1u);
+                  umma_tf32(d, dah, dbl, idesc, 1u);
+                  umma_tf32(d, dal, dbh, idesc, 1u);
+                }
+              }
+              umma_commit(&bempty[sb]);
+            }
+            umma_commit(&aempty[sa]);
           }
-          tc_fence_after();
-          cnn_mma_block(ring, s, tmem + (uint32_t)(ab * bn), idesc, kb == 0);
-          umma_commit(&empty[s]);
-        }
         if (ok) umma_commit(&tfull[ab]);
       }
-      umma_commit(done);  // always: teardown after an abort waits for the MMAs in flight
+      umma_commit(done);  // always: teardown waits for the MMAs in flight
     }
   } else {
     const int q = warp & 3;
     const uint32_t lane_addr = (uint32_t)(q * 32) << 16;
-    // TMEM lane = pixel h*16 + w of the 8 x 16 block: a warp holds rows 2q, 2q+1
+    // TMEM lane = pixel h*16 + w of an 8 x 16 block: a warp holds rows 2q, 2q+1
     const int h = 2 * q + (lane >> 4), w = lane & 15;
     const bool owner = (lane & 17) == 0;
     const int so = p.side / 2, pad = p.out_pad, hp = so + 2 * pad;
@@ -428,35 +487,38 @@ __global__ void __launch_bounds__(CNN_THREADS) cnn_conv_kernel(
     const long long plane = (long long)p.batch * img_elems;
     int local = 0;
     for (int t = blockIdx.x; t < p.total_tiles; t += gridDim.x, ++local) {
-      const int ab = local & 1;
-      const bool waited = mbar_wait_bounded(&tfull[ab], (uint32_t)((local >> 1) & 1), abort_flag,
-                                            p.err, CNN_TIMEOUT_NS) && !*abort_flag;
+      const int ab = local % p.nbuf, use = local / p.nbuf;
+      const bool waited = mbar_wait_bounded(&tfull[ab], (uint32_t)(use & 1), abort_flag, p.err,
+                                            CNN_TIMEOUT_NS) && !*abort_flag;
       if (!__all_sync(0xffffffffu, waited)) break;
       tc_fence_after();
       int model, img, y0, x0;
       decode(t, model, img, y0, x0);
-      const int py = (y0 + h) >> 1, px = (x0 + w) >> 1;
       float* base = p.out + (long long)model * 2 * plane + (long long)img * img_elems;
       const float* bias = s_vec + model * bn;
       const float* scale = bias + nvec;
       const float* shift = scale + nvec;
-      for (int c0 = 0; c0 < p.cout; c0 += 16) {
-        uint32_t v[16];
-        tmem_ld16(tmem + lane_addr + (uint32_t)(ab * bn + c0), v);
-        tmem_ld_wait();
-        float hi[16], lo[16];
+      for (int m = 0; m < mt; ++m) {
+        const int py = (y0 + 8 * m + h) >> 1, px = (x0 + w) >> 1;
+        const uint32_t col = (uint32_t)((ab * mt + m) * bn);
+        for (int c0 = 0; c0 < p.cout; c0 += 16) {
+          uint32_t v[16];
+          tmem_ld16(tmem + lane_addr + col + (uint32_t)c0, v);
+          tmem_ld_wait();
+          float hi[16], lo[16];
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          float f = __uint_as_float(v[j]);
-          f = fmaxf(f, __shfl_xor_sync(0xffffffffu, f, 1));
-          f = fmaxf(f, __shfl_xor_sync(0xffffffffu, f, 16));
-          const int c = c0 + j;
-          const float y = fmaxf(f + bias[c], 0.0f) * scale[c] + shift[c];
-          split_tf32f(y, hi[j], lo[j]);
+          for (int j = 0; j < 16; ++j) {
+            float f = __uint_as_float(v[j]);
+            f = fmaxf(f, __shfl_xor_sync(0xffffffffu, f, 1));
+            f = fmaxf(f, __shfl_xor_sync(0xffffffffu, f, 16));
+            const int c = c0 + j;
+            const float y = fmaxf(f + bias[c], 0.0f) * scale[c] + shift[c];
+            split_tf32f(y, hi[j], lo[j]);
+          }
+          if (owner) cnn_store16(base, plane, so, pad, p.cout, py, px, c0, hi, lo);
         }
-        if (owner) cnn_store16(base, plane, so, pad, p.cout, py, px, c0, hi, lo);
       }
-      // this warp's TMEM reads are complete: hand the accumulator back
+      // this warp's TMEM reads are complete: hand the accumulator set back
       tc_fence_before();
       __syncwarp();
       if (lane == 0)
@@ -474,6 +536,29 @@ __global__ void __launch_bounds__(CNN_THREADS) cnn_conv_kernel(
   }
 }
 
+// Conv stage plan: two accumulator sets (the epilogue of one tile overlaps
+// the MMAs of the next), mt = 2 blocks per tile (each weight tile serves 256
+// pixels) when TMEM holds 2 x 2 x cout columns, else 1; ring depths from a
+// shared-memory budget (two CTAs per SM for the small layers).
+struct CnnConvPlan {
+  int mt, nbuf, a_stages, b_stages;
+  size_t smem;
+};
+static CnnConvPlan cnn_conv_plan(int cout, int models) {
+  CnnConvPlan c;
+  c.nbuf = 2;
+  c.mt = 2 * 2 * cout <= 512 ? 2 : 1;
+  const size_t a = 2 * (size_t)cnn_conv_a_plane(c.mt), b = 2 * (size_t)cout * CNN_BK * 4;
+  const size_t fixed = 1024 + 512 + (size_t)12 * models * cout;  // align slack, barriers, table
+  const size_t budget = cout <= 64 ? 110 * 1024 : 222 * 1024;
+  c.a_stages = 2;
+  size_t rest = budget - fixed - c.a_stages * a;
+  int bs = (int)(rest / b);
+  c.b_stages = bs < 2 ? 2 : (bs > 8 ? 8 : bs);
+  c.smem = fixed + c.a_stages * a + c.b_stages * b;
+  return c;
+}
+
 struct CnnFcArgs {
   int models, batch;
   int bn, nkb, stages;
@@ -482,9 +567,14 @@ struct CnnFcArgs {
   int* err;
 };
 
-// Split-K fully connected layer: A = weight planes [2M][rows][K] (128 rows per
+// Split-K fully connected layer: A = fp32 weights [M][rows][K] (128 rows per
 // CTA), B = activation planes [2M][batch][K] (bn masks per CTA), K range
 // split blockIdx.y % nsplit; FP32 partial sums to part[split][model][mask][row].
+// The TMA writes the fp32 weight tile into the stage's hi tile; warps 2..5
+// split it in place (hi) and into the lo tile (same swizzled positions:
+// the transform is elementwise), fence the generic-proxy writes for the
+// tensor core and arrive on conv[s]; the MMA warp waits on conv[s].  After
+// the K loop the same warps run the epilogue.
 __global__ void __launch_bounds__(CNN_THREADS) cnn_fc_kernel(
     const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
     CnnFcArgs p) {
@@ -493,7 +583,8 @@ __global__ void __launch_bounds__(CNN_THREADS) cnn_fc_kernel(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
   CnnRing ring{smem, 2 * CNN_A_TILE + 2 * p.bn * CNN_BK * 4, p.bn * CNN_BK * 4};
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + p.stages * ring.stage_bytes);
-  uint64_t* empty = full + p.stages;
+  uint64_t* conv = full + p.stages;
+  uint64_t* empty = conv + p.stages;
   uint64_t* accum = empty + p.stages;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accum + 1);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
@@ -508,6 +599,7 @@ __global__ void __launch_bounds__(CNN_THREADS) cnn_fc_kernel(
   if (threadIdx.x == 0) {
     for (int s = 0; s < p.stages; ++s) {
       mbar_init(&full[s], 1);
+      mbar_init(&conv[s], 4);
       mbar_init(&empty[s], 1);
     }
     mbar_init(accum, 1);
@@ -529,10 +621,9 @@ __global__ void __launch_bounds__(CNN_THREADS) cnn_fc_kernel(
         const int s = kb % p.stages;
         const uint32_t ph = (uint32_t)((kb / p.stages) & 1);
         if (!mbar_wait_bounded(&empty[s], ph ^ 1u, abort_flag, p.err, CNN_TIMEOUT_NS)) break;
-        mbar_expect_tx(&full[s], (uint32_t)ring.stage_bytes);
+        mbar_expect_tx(&full[s], (uint32_t)(CNN_A_TILE + 2 * ring.b_bytes));
         const int k0 = (split * nkb + kb) * CNN_BK;
-        for (int pl = 0; pl < 2; ++pl)
-          tma_load_3d(ring.a(s, pl), &tmA, k0, m0, 2 * model + pl, &full[s]);
+        tma_load_3d(ring.a(s, 0), &tmA, k0, m0, model, &full[s]);
         for (int pl = 0; pl < 2; ++pl)
           tma_load_3d(ring.b(s, pl), &tmB, k0, n0, 2 * model + pl, &full[s]);
         issued = kb + 1;
@@ -548,7 +639,7 @@ __global__ void __launch_bounds__(CNN_THREADS) cnn_fc_kernel(
       for (int kb = 0; kb < nkb; ++kb) {
         const int s = kb % p.stages;
         const uint32_t ph = (uint32_t)((kb / p.stages) & 1);
-        if (!mbar_wait_bounded(&full[s], ph, abort_flag, p.err, CNN_TIMEOUT_NS)) break;
+        if (!mbar_wait_bounded(&conv[s], ph, abort_flag, p.err, CNN_TIMEOUT_NS)) break;
         tc_fence_after();
         cnn_mma_block(ring, s, tmem, idesc, kb == 0);
         umma_commit(&empty[s]);
@@ -556,6 +647,33 @@ __global__ void __launch_bounds__(CNN_THREADS) cnn_fc_kernel(
       umma_commit(accum);
     }
   } else {
+    // weight split: 2048 fp32 of the stage's A tile, 16 per thread
+    const int et = threadIdx.x - 64;  // 0..127
+    for (int kb = 0; kb < nkb; ++kb) {
+      const int s = kb % p.stages;
+      const uint32_t ph = (uint32_t)((kb / p.stages) & 1);
+      const bool got = mbar_wait_bounded(&full[s], ph, abort_flag, p.err, CNN_TIMEOUT_NS);
+      if (!__all_sync(0xffffffffu, got)) break;
+      float4* hi = reinterpret_cast<float4*>(ring.a(s, 0));
+      float4* lo = reinterpret_cast<float4*>(ring.a(s, 1));
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int i = et + 128 * u;
+        const float4 x = hi[i];
+        float4 h, l;
+        split_tf32f(x.x, h.x, l.x);
+        split_tf32f(x.y, h.y, l.y);
+        split_tf32f(x.z, h.z, l.z);
+        split_tf32f(x.w, h.w, l.w);
+        hi[i] = h;
+        lo[i] = l;
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      __syncwarp();
+      if (lane == 0)
+        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&conv[s]))
+                     : "memory");
+    }
     const int q = warp & 3;
     const bool waited =
         mbar_wait_bounded(accum, 0u, abort_flag, p.err, CNN_TIMEOUT_NS) && !*abort_flag;
@@ -660,8 +778,8 @@ static int cnn_launch(Kern kernel, dim3 grid, size_t smem, const CUtensorMap& ta
 
 // persistent grid of the conv kernel: resident CTAs per SM by shared memory
 // (with the 1 KB the runtime reserves per CTA) and registers, capped by TMEM
-// (two accumulators of cout columns each, allocated as a power of two)
-static int cnn_conv_grid(int total, int cout, size_t smem) {
+// (tmem_cols accumulator columns, allocated as a power of two)
+static int cnn_conv_grid(int total, int tmem_cols, size_t smem) {
   static int done[64];
   int dev = 0, nsm = 148, sm_smem = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return -1;
@@ -683,7 +801,7 @@ static int cnn_conv_grid(int total, int cout, size_t smem) {
   const int regs = ((fa.numRegs + 7) / 8) * 8 * CNN_THREADS;
   if (regs > 0 && occ > 65536 / regs) occ = 65536 / regs;
   int tcols = 32;
-  while (tcols < 2 * cout) tcols <<= 1;
+  while (tcols < tmem_cols) tcols <<= 1;
   if (occ > 512 / tcols) occ = 512 / tcols;
   if (occ < 1) occ = 1;
   const long long g = (long long)nsm * occ;
@@ -753,7 +871,7 @@ extern "C" int euv_cnn_pack(int n_models, const euv_cnn_model_weights* w, int ma
     }
     const long long n1 = (long long)CNN_FC1_N * CNN_FC1_K;
     cnn_pack_fc_kernel<<<(unsigned)((n1 + 255) / 256), 256, 0, stream>>>(
-        CNN_FC1_N, CNN_FC1_N, CNN_FC1_K, 1, mw.fc1_w, blob + L.fc1 + (size_t)m * 2 * n1);
+        CNN_FC1_N, CNN_FC1_N, CNN_FC1_K, 1, mw.fc1_w, blob + L.fc1 + (size_t)m * n1);
     EUV_LAUNCH_CHECK();
     cnn_pack_vec_kernel<<<CNN_FC1_N / 256, 256, 0, stream>>>(
         CNN_FC1_N, CNN_FC1_N, mw.fc1_b, nullptr, nullptr, nullptr, nullptr, 0.0,
@@ -761,7 +879,7 @@ extern "C" int euv_cnn_pack(int n_models, const euv_cnn_model_weights* w, int ma
     EUV_LAUNCH_CHECK();
     const long long n2 = (long long)L.op * CNN_FC1_N;
     cnn_pack_fc_kernel<<<(unsigned)((n2 + 255) / 256), 256, 0, stream>>>(
-        mw.n_out, L.op, CNN_FC1_N, 0, mw.fc2_w, blob + L.fc2 + (size_t)m * 2 * n2);
+        mw.n_out, L.op, CNN_FC1_N, 0, mw.fc2_w, blob + L.fc2 + (size_t)m * n2);
     EUV_LAUNCH_CHECK();
     cnn_pack_vec_kernel<<<(L.op + 255) / 256, 256, 0, stream>>>(
         mw.n_out, L.op, mw.fc2_b, nullptr, nullptr, nullptr, nullptr, 0.0,
@@ -832,7 +950,8 @@ extern "C" int euv_cnn_predict(const euv_cnn_desc* d, const uint8_t* d_bits, con
     const cuuint64_t adims[5] = {(cuuint64_t)ci, sp, sp, (cuuint64_t)B, (cuuint64_t)2 * M};
     const cuuint64_t astr[4] = {(cuuint64_t)ci * 4, sp * ci * 4, sp * sp * ci * 4,
                                 (cuuint64_t)B * sp * sp * ci * 4};
-    const cuuint32_t abox[5] = {CNN_BK, 16, 8, 1, 1};
+    const CnnConvPlan cp = cnn_conv_plan(co, M);
+    const cuuint32_t abox[5] = {CNN_BK, 16, (cuuint32_t)(8 * cp.mt + 2), 1, 1};
     int rc = make_map_f32(&ta, in, 5, adims, astr, abox);
     if (rc) return rc;
     const cuuint64_t bdims[3] = {(cuuint64_t)9 * ci, (cuuint64_t)co, (cuuint64_t)2 * M};
@@ -841,29 +960,31 @@ extern "C" int euv_cnn_predict(const euv_cnn_desc* d, const uint8_t* d_bits, con
     rc = make_map_f32(&tb, const_cast<float*>(blob + L.w[l]), 3, bdims, bstr, bbox);
     if (rc) return rc;
     CnnConvArgs p = {};
+    p.models = M;
     p.batch = B;
     p.side = S;
     p.tiles_x = S / 16;
-    p.tiles_img = (S / 8) * (S / 16);
+    p.tiles_img = (S / (8 * cp.mt)) * (S / 16);
     const long long total = (long long)M * B * p.tiles_img;
     if (total > 0x7fffffffLL) {
       euv_set_error("euv_cnn_predict: too many conv tiles (%lld)", total);
       return EUV_ERR_BAD_ARG;
     }
     p.total_tiles = (int)total;
-    p.models = M;
     p.cin = ci;
     p.cout = co;
-    p.nkb = 9 * ci / CNN_BK;
-    p.stages = cnn_stages(co);
+    p.mt = cp.mt;
+    p.nbuf = cp.nbuf;
+    p.a_stages = cp.a_stages;
+    p.b_stages = cp.b_stages;
     p.out_pad = l < 4 ? 1 : 0;
     p.bias = blob + L.bias[l];
     p.scale = blob + L.scale[l];
     p.shift = blob + L.shift[l];
     p.out = work + W.act[l];
     p.err = err;
-    const size_t smem = cnn_smem(co, p.stages) + (size_t)12 * M * co;
-    const int grid = cnn_conv_grid(p.total_tiles, co, smem);
+    const size_t smem = cp.smem;
+    const int grid = cnn_conv_grid(p.total_tiles, cp.nbuf * cp.mt * co, smem);
     if (grid < 1) {
       euv_set_error("euv_cnn_predict: conv kernel setup failed");
       return EUV_ERR_CUDA;
@@ -881,7 +1002,7 @@ extern "C" int euv_cnn_predict(const euv_cnn_desc* d, const uint8_t* d_bits, con
     float* wa = const_cast<float*>(blob + (f == 0 ? L.fc1 : L.fc2));
     float* act = work + (f == 0 ? W.act[4] : W.h);
     CUtensorMap ta, tb;
-    const cuuint64_t adims[3] = {(cuuint64_t)K, (cuuint64_t)rows, (cuuint64_t)2 * M};
+    const cuuint64_t adims[3] = {(cuuint64_t)K, (cuuint64_t)rows, (cuuint64_t)M};
     const cuuint64_t astr[2] = {(cuuint64_t)K * 4, (cuuint64_t)rows * K * 4};
     const cuuint32_t abox[3] = {CNN_BK, 128, 1};
     int rc = make_map_f32(&ta, wa, 3, adims, astr, abox);

@@ -223,7 +223,7 @@ def _cnn(a) -> dict:
             "masks_per_s": a.clips / (ms / 1e3),
             "fp32_equiv_tflops": flop / (ms / 1e3) / 1e12,
             "tf32_tensor_tflops": 3 * (flop - conv1) / (ms / 1e3) / 1e12,
-            "fc1_weight_planes_gb": len(n_outs) * 2 * 4096 * 65536 * 4 / 1e9}
+            "fc1_weight_gb": len(n_outs) * 4096 * 65536 * 4 / 1e9}
 
 
 def _time(fn, reps: int) -> float:

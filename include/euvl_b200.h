@@ -177,7 +177,8 @@ int euv_mask_raster(int n_masks, int ndivx, int ndivy, int n_rects, const int* d
  * 512 x 512 input, fc1 65536 -> 4096 + ReLU, fc2 4096 -> n_out.  Weights are
  * the torch tensors of a state_dict, fp32, contiguous, on the device, in torch
  * layout (conv [cout][cin][3][3], linear [out][in]); euv_cnn_pack rewrites
- * them once into a blob of TF32 (hi, lo) planes (about 2.2 GB per model).
+ * them once into a blob (conv weights as TF32 (hi, lo) planes, fc weights
+ * fp32 in the kernels' K order; about 1.1 GB per model).
  * The predict takes mask.bin rasters (2048 x 2048 bits, MSB first, 524288
  * bytes per mask), and writes out[model][mask][j] = fc2 output / factor
  * (the division of predict.py:114-119, in double) for j < n_out[model],

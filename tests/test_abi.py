@@ -67,8 +67,8 @@ def test_cnn_entry_points_reject_bad_arguments(lib):
     assert lib.euv_cnn_blob_bytes(7, 1901) == 0
     assert lib.euv_cnn_blob_bytes(6, L.EUV_CNN_MAX_OUT + 1) == 0
     assert lib.euv_cnn_workspace_bytes(6, 0, 1901) == 0
-    # 6 networks: fc1 planes dominate (2 x 4096 x 65536 fp32 each)
-    assert lib.euv_cnn_blob_bytes(6, 1901) > 6 * 2 * 4096 * 65536 * 4
+    # 6 networks: the fp32 fc1 weights dominate (4096 x 65536 each)
+    assert lib.euv_cnn_blob_bytes(6, 1901) > 6 * 4096 * 65536 * 4
     d = L.CnnDesc()
     d.n_models, d.n_masks, d.max_out = 1, 1, 10
     d.n_out[0] = 11  # above max_out
