@@ -20,6 +20,9 @@
 
 namespace euv {
 
+int zgemm_sub(int m, int n, int k, const double2* a, long long lda, long long sa,
+              const double2* b, long long ldb, long long sb, double2* c, long long ldc,
+              long long sc, int batch, cudaStream_t stream);
 int zgemm(int m, int n, int k, cplx alpha, const double* scale, const double2* a, long long lda,
           long long sa, const double2* b, long long ldb, long long sb, cplx beta, double2* c,
           long long ldc, long long sc, cplx diag, int batch, const int* steps, int step,
@@ -476,9 +479,9 @@ static int lu_update(int n, int j0, int jb, int c0, int nc, double2* A, long lon
                                            A + j0 + (long long)c0 * lda, lda, sa);
   EUV_LAUNCH_CHECK();
   const int rest = n - j0 - jb;
-  return zgemm(rest, nc, jb, mk(-1.0, 0.0), nullptr, A + (j0 + jb) + (long long)j0 * lda, lda, sa,
-               A + j0 + (long long)c0 * lda, lda, sa, mk(1.0, 0.0),
-               A + (j0 + jb) + (long long)c0 * lda, lda, sa, mk(0.0, 0.0), batch, nullptr, 0, st);
+  return zgemm_sub(rest, nc, jb, A + (j0 + jb) + (long long)j0 * lda, lda, sa,
+                   A + j0 + (long long)c0 * lda, lda, sa, A + (j0 + jb) + (long long)c0 * lda,
+                   lda, sa, batch, st);
 }
 
 // Right-looking LU with one panel of look-ahead: after panel j, its update of
@@ -738,9 +741,8 @@ int lu_solve(int n, int nrhs, const double2* LU, long long lda, long long sa, co
     EUV_LAUNCH_CHECK();
     const int rest = n - j0 - jb;
     if (rest > 0) {
-      int rc = zgemm(rest, nrhs, jb, mk(-1.0, 0.0), nullptr, LU + (j0 + jb) + (long long)j0 * lda,
-                     lda, sa, B + j0, ldb, sb, mk(1.0, 0.0), B + j0 + jb, ldb, sb, mk(0.0, 0.0),
-                     batch, nullptr, 0, stream);
+      int rc = zgemm_sub(rest, nrhs, jb, LU + (j0 + jb) + (long long)j0 * lda, lda, sa, B + j0,
+                         ldb, sb, B + j0 + jb, ldb, sb, batch, stream);
       if (rc != EUV_OK) return rc;
     }
   }
@@ -753,9 +755,8 @@ int lu_solve(int n, int nrhs, const double2* LU, long long lda, long long sa, co
                                                   sa, B + j0, ldb, sb);
     EUV_LAUNCH_CHECK();
     if (j0 > 0) {
-      int rc = zgemm(j0, nrhs, jb, mk(-1.0, 0.0), nullptr, LU + (long long)j0 * lda, lda, sa,
-                     B + j0, ldb, sb, mk(1.0, 0.0), B, ldb, sb, mk(0.0, 0.0), batch, nullptr, 0,
-                     stream);
+      int rc = zgemm_sub(j0, nrhs, jb, LU + (long long)j0 * lda, lda, sa, B + j0, ldb, sb, B,
+                         ldb, sb, batch, stream);
       if (rc != EUV_OK) return rc;
     }
   }

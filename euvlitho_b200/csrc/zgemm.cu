@@ -54,12 +54,19 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
                : "d"(a), "d"(b));
 }
 
-__global__ void __launch_bounds__(GTHREADS, 2) zgemm_kernel(GemmArgs p) {
+// UPD: C -= A B (alpha, beta, scale, diag ignored).  The accumulators start
+// from C, whose loads are issued right after the first operand copies, and the
+// A fragments are negated: no read of C after the products.
+// MI: 8-row blocks per warp (tile BM = 16 MI rows x 64 columns); ST: cp.async stages.
+template <bool UPD, int MI, int ST>
+__global__ void __launch_bounds__(GTHREADS, MI == 2 ? 4 : 2) zgemm_kernel(GemmArgs p) {
+  constexpr int BM = 16 * MI;
+  constexpr int AP = BM + 2;
   extern __shared__ double2 smem[];
   double2* As = smem;
-  double2* Bs = smem + GSTAGES * GBK * APAD;
+  double2* Bs = smem + ST * GBK * AP;
   const int bz = blockIdx.z;
-  const int m0 = blockIdx.x * GBM;
+  const int m0 = blockIdx.x * BM;
   const int n0 = blockIdx.y * GBN;
   const double2* A = p.a + (long long)bz * p.sa;
   const double2* B = p.b + (long long)bz * p.sb;
@@ -70,30 +77,30 @@ __global__ void __launch_bounds__(GTHREADS, 2) zgemm_kernel(GemmArgs p) {
     // inactive double-angle step for this batch entry: C = A
     // eight loads in flight per thread before their stores
     constexpr int U = 8;
-    for (int base = 0; base < GBM * GBN; base += GTHREADS * U) {
+    for (int base = 0; base < BM * GBN; base += GTHREADS * U) {
       double2 v[U];
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         const int idx = base + tid + u * GTHREADS;
-        const int gi = m0 + idx % GBM, gj = n0 + idx / GBM;
-        v[u] = (idx < GBM * GBN && gi < p.m && gj < p.n) ? A[gi + (long long)gj * p.lda]
+        const int gi = m0 + idx % BM, gj = n0 + idx / BM;
+        v[u] = (idx < BM * GBN && gi < p.m && gj < p.n) ? A[gi + (long long)gj * p.lda]
                                                          : make_double2(0.0, 0.0);
       }
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         const int idx = base + tid + u * GTHREADS;
-        const int gi = m0 + idx % GBM, gj = n0 + idx / GBM;
-        if (idx < GBM * GBN && gi < p.m && gj < p.n) C[gi + (long long)gj * p.ldc] = v[u];
+        const int gi = m0 + idx % BM, gj = n0 + idx / BM;
+        if (idx < BM * GBN && gi < p.m && gj < p.n) C[gi + (long long)gj * p.ldc] = v[u];
       }
     }
     return;
   }
 
   const int warp = tid >> 5, lane = tid & 31;
-  const int wm = (warp & 1) * 32, wn = (warp >> 1) * 32;
-  double accr[4][4][2], acci[4][4][2];
+  const int wm = (warp & 1) * (8 * MI), wn = (warp >> 1) * 32;
+  double accr[MI][4][2], acci[MI][4][2];
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < MI; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       accr[i][j][0] = accr[i][j][1] = 0.0;
@@ -103,16 +110,16 @@ __global__ void __launch_bounds__(GTHREADS, 2) zgemm_kernel(GemmArgs p) {
   const int ktiles = (p.k + GBK - 1) / GBK;
   auto load_tile = [&](int stage, int kt) {
     const int k0 = kt * GBK;
-    double2* as = As + stage * GBK * APAD;
+    double2* as = As + stage * GBK * AP;
     double2* bs = Bs + stage * GBK * BPAD;
 #pragma unroll
-    for (int r = 0; r < (GBM * GBK) / GTHREADS; ++r) {
+    for (int r = 0; r < (BM * GBK) / GTHREADS; ++r) {
       int idx = tid + r * GTHREADS;
-      int i = idx % GBM, kk = idx / GBM;
+      int i = idx % BM, kk = idx / BM;
       int gi = m0 + i, gk = k0 + kk;
       bool ok = gi < p.m && gk < p.k;
       const double2* src = ok ? A + gi + (long long)gk * p.lda : A;
-      cp_async16(&as[kk * APAD + i], src, ok);
+      cp_async16(&as[kk * AP + i], src, ok);
     }
 #pragma unroll
     for (int r = 0; r < (GBN * GBK) / GTHREADS; ++r) {
@@ -126,27 +133,47 @@ __global__ void __launch_bounds__(GTHREADS, 2) zgemm_kernel(GemmArgs p) {
   };
 
 #pragma unroll
-  for (int s = 0; s < GSTAGES - 1; ++s) {
+  for (int s = 0; s < ST - 1; ++s) {
     if (s < ktiles) load_tile(s, s);
     cp_async_commit();
   }
+  if (UPD) {
+#pragma unroll
+    for (int mi = 0; mi < MI; ++mi) {
+      const int row = m0 + wm + mi * 8 + (lane >> 2);
+#pragma unroll
+      for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int col = n0 + wn + ni * 8 + (lane & 3) * 2 + e;
+          const double2 v = (row < p.m && col < p.n) ? C[row + (long long)col * p.ldc]
+                                                     : make_double2(0.0, 0.0);
+          accr[mi][ni][e] = v.x;
+          acci[mi][ni][e] = v.y;
+        }
+    }
+  }
   for (int kt = 0; kt < ktiles; ++kt) {
-    cp_async_wait<GSTAGES - 2>();
+    cp_async_wait<ST - 2>();
     __syncthreads();
     {
-      int nk = kt + GSTAGES - 1;
-      if (nk < ktiles) load_tile(nk % GSTAGES, nk);
+      int nk = kt + ST - 1;
+      if (nk < ktiles) load_tile(nk % ST, nk);
       cp_async_commit();
     }
-    const double2* as = As + (kt % GSTAGES) * GBK * APAD;
-    const double2* bs = Bs + (kt % GSTAGES) * GBK * BPAD;
+    const double2* as = As + (kt % ST) * GBK * AP;
+    const double2* bs = Bs + (kt % ST) * GBK * BPAD;
 #pragma unroll
     for (int ks = 0; ks < GBK; ks += 4) {
       const int kk = ks + (lane & 3);
-      double ar[4], ai[4], an[4], br[4], bi[4];
+      double ar[MI], ai[MI], an[MI], br[4], bi[4];
 #pragma unroll
-      for (int mi = 0; mi < 4; ++mi) {
-        double2 v = as[kk * APAD + wm + mi * 8 + (lane >> 2)];
+      for (int mi = 0; mi < MI; ++mi) {
+        double2 v = as[kk * AP + wm + mi * 8 + (lane >> 2)];
+        if (UPD) {
+          v.x = -v.x;
+          v.y = -v.y;
+        }
         ar[mi] = v.x;
         ai[mi] = v.y;
         an[mi] = -v.y;
@@ -158,7 +185,7 @@ __global__ void __launch_bounds__(GTHREADS, 2) zgemm_kernel(GemmArgs p) {
         bi[ni] = v.y;
       }
 #pragma unroll
-      for (int mi = 0; mi < 4; ++mi)
+      for (int mi = 0; mi < MI; ++mi)
 #pragma unroll
         for (int ni = 0; ni < 4; ++ni) {
           dmma(accr[mi][ni][0], accr[mi][ni][1], ar[mi], br[ni]);
@@ -170,13 +197,29 @@ __global__ void __launch_bounds__(GTHREADS, 2) zgemm_kernel(GemmArgs p) {
   }
   cp_async_wait<0>();
 
+  if (UPD) {
+#pragma unroll
+    for (int mi = 0; mi < MI; ++mi) {
+      const int row = m0 + wm + mi * 8 + (lane >> 2);
+#pragma unroll
+      for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int col = n0 + wn + ni * 8 + (lane & 3) * 2 + e;
+          if (row < p.m && col < p.n)
+            C[row + (long long)col * p.ldc] = make_double2(accr[mi][ni][e], acci[mi][ni][e]);
+        }
+    }
+    return;
+  }
+
   const double sc = p.scale ? p.scale[bz] : 1.0;
   const cplx alpha = mk(p.alpha.x * sc, p.alpha.y * sc);
   const cplx beta = mk(p.beta.x, p.beta.y);
   const bool use_beta = (p.beta.x != 0.0 || p.beta.y != 0.0);
   const cplx dg = mk(p.diag.x, p.diag.y);
 #pragma unroll
-  for (int mi = 0; mi < 4; ++mi) {
+  for (int mi = 0; mi < MI; ++mi) {
     const int row = m0 + wm + mi * 8 + (lane >> 2);
     // the 8 reads of C for this row block are issued before its stores (a
     // load after a store through the same pointer type would wait for it)
@@ -204,14 +247,53 @@ __global__ void __launch_bounds__(GTHREADS, 2) zgemm_kernel(GemmArgs p) {
   }
 }
 
-int zgemm_launch(const GemmArgs& p, int batch, cudaStream_t stream) {
+template <int MI, int ST>
+constexpr size_t zgemm_smem() {
+  return (size_t)ST * GBK * (16 * MI + 2 + BPAD) * sizeof(double2);
+}
+
+int zgemm_launch(const GemmArgs& p, int batch, cudaStream_t stream, bool upd = false) {
   if (p.m <= 0 || p.n <= 0 || batch <= 0) return EUV_OK;
-  static int smem_done[64];
-  EUV_CUDA_TRY(ensure_smem(zgemm_kernel, (int)GSMEM, smem_done));
-  dim3 grid((p.m + GBM - 1) / GBM, (p.n + GBN - 1) / GBN, batch);
-  zgemm_kernel<<<grid, GTHREADS, GSMEM, stream>>>(p);
+  static int smem_done[64], smem_done_upd[64], smem_done_rk[64];
+  if (upd && p.k <= 2 * GBK) {
+    // rank-k update with k <= 32 (the LU's trailing updates): 32 x 64 tiles and
+    // two stages (both k tiles in flight at once) for four CTAs per SM
+    constexpr size_t sm = zgemm_smem<2, 2>();
+    dim3 grid((p.m + 31) / 32, (p.n + GBN - 1) / GBN, batch);
+    EUV_CUDA_TRY(ensure_smem(zgemm_kernel<true, 2, 2>, (int)sm, smem_done_rk));
+    zgemm_kernel<true, 2, 2><<<grid, GTHREADS, sm, stream>>>(p);
+  } else if (upd) {
+    constexpr size_t sm = zgemm_smem<4, GSTAGES>();
+    dim3 grid((p.m + GBM - 1) / GBM, (p.n + GBN - 1) / GBN, batch);
+    EUV_CUDA_TRY(ensure_smem(zgemm_kernel<true, 4, GSTAGES>, (int)sm, smem_done_upd));
+    zgemm_kernel<true, 4, GSTAGES><<<grid, GTHREADS, sm, stream>>>(p);
+  } else {
+    dim3 grid((p.m + GBM - 1) / GBM, (p.n + GBN - 1) / GBN, batch);
+    EUV_CUDA_TRY(ensure_smem(zgemm_kernel<false, 4, GSTAGES>, (int)GSMEM, smem_done));
+    zgemm_kernel<false, 4, GSTAGES><<<grid, GTHREADS, GSMEM, stream>>>(p);
+  }
   EUV_LAUNCH_CHECK();
   return EUV_OK;
+}
+
+// C -= A B (the rank-k updates of the blocked LU and its solves)
+int zgemm_sub(int m, int n, int k, const double2* a, long long lda, long long sa,
+              const double2* b, long long ldb, long long sb, double2* c, long long ldc,
+              long long sc, int batch, cudaStream_t stream) {
+  GemmArgs p = {};
+  p.m = m;
+  p.n = n;
+  p.k = k;
+  p.a = a;
+  p.lda = lda;
+  p.sa = sa;
+  p.b = b;
+  p.ldb = ldb;
+  p.sb = sb;
+  p.c = c;
+  p.ldc = ldc;
+  p.sc = sc;
+  return zgemm_launch(p, batch, stream, true);
 }
 
 int zgemm(int m, int n, int k, cplx alpha, const double* scale, const double2* a, long long lda,
