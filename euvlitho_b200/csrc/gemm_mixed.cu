@@ -46,6 +46,8 @@ constexpr int MX_THREADS = 192;
 constexpr int MX_TMEM_COLS = 512;
 constexpr size_t MX_SMEM = (size_t)MX_STAGES * MX_STAGE_BYTES + 1024 + 256;
 constexpr unsigned long long MX_TIMEOUT_NS = 2000000000ull;
+// stage slot of each B plane (gmem order Re_hi, Re_lo, Im_hi, Im_lo)
+__device__ constexpr int kBSlot[4] = {0, 2, 1, 3};
 
 struct MixedArgs {
   int m, n, kp;
@@ -149,8 +151,10 @@ __global__ void __launch_bounds__(MX_THREADS, 1)
         const int k0 = kb * MX_BK;
         for (int pl = 0; pl < MX_PLANES; ++pl)
           tma_load_3d(a_tile(s, pl), &tmA, k0, m0, b * MX_PLANES + pl, &full[s]);
+        // B planes in the stage as Re_hi, Im_hi, Re_lo, Im_lo: [Br | Bi] of a
+        // precision level are adjacent, one N = 256 operand
         for (int pl = 0; pl < MX_PLANES; ++pl)
-          tma_load_3d(b_tile(s, pl), &tmB, k0, n0, b * MX_PLANES + pl, &full[s]);
+          tma_load_3d(b_tile(s, kBSlot[pl]), &tmB, k0, n0, b * MX_PLANES + pl, &full[s]);
         issued = kb + 1;
       }
       if (*abort_flag) {
@@ -170,11 +174,17 @@ __global__ void __launch_bounds__(MX_THREADS, 1)
       // error is the same for TF32-exact operands and grows linearly in K), so
       // the K range is split in two halves with their own Re/Im accumulators,
       // summed in FP64 by the epilogue.
-      // Products (A plane, B plane): Re = +ArBr -AiBi, Im = +ArBi +AiBr, each
-      // as hi*hi + hi*lo + lo*hi; the Re list's last three are negated.
-      const int re_a[6] = {0, 0, 1, 2, 2, 3}, re_b[6] = {0, 1, 0, 2, 3, 2};
-      const int im_a[6] = {0, 0, 1, 2, 2, 3}, im_b[6] = {2, 3, 2, 0, 1, 0};
+      // Products: Re = +ArBr -AiBi, Im = +ArBi +AiBr, each as hi*hi + hi*lo +
+      // lo*hi.  The Ar terms of Re and Im share their A operand: one MMA of
+      // N = 256 against [Br | Bi] (adjacent in the stage) writes both
+      // accumulators (Re and Im of a K half are adjacent TMEM columns); the Ai
+      // terms differ in sign and take two N = 128 MMAs each (Re negated).
+      // A planes: 0 Re_hi 1 Re_lo 2 Im_hi 3 Im_lo; B stage slots: kBSlot.
+      const int ar_a[3] = {0, 0, 1}, ar_b[3] = {0, 2, 0};  // B slot of [Br|Bi] hi / lo
+      const int ai_a[3] = {2, 2, 3};
+      const int ai_bi[3] = {1, 3, 1}, ai_br[3] = {0, 2, 0};  // slots of Bi / Br
       const uint32_t id_pos = idesc_tf32(false), id_neg = idesc_tf32(true);
+      const uint32_t id_wide = idesc_tf32_mn(false, MX_BM, 2 * MX_BN);
       const int half = (nkb + 1) / 2;  // k-blocks [0, half) -> set 0, [half, nkb) -> set 1
       for (int kb = 0; kb < nkb; ++kb) {
         const int s = kb % MX_STAGES;
@@ -189,12 +199,16 @@ __global__ void __launch_bounds__(MX_THREADS, 1)
         for (int k8 = 0; k8 < MX_BK / 8; ++k8) {
           const uint32_t first = (kb != kb0 || k8) ? 1u : 0u;
 #pragma unroll
-          for (int q = 0; q < 6; ++q) {
-            umma_tf32(t_re, umma_desc_sw64(a_tile(s, re_a[q]) + k8 * 32),
-                      umma_desc_sw64(b_tile(s, re_b[q]) + k8 * 32), q >= 3 ? id_neg : id_pos,
+          for (int q = 0; q < 3; ++q)
+            umma_tf32(t_re, umma_desc_sw64(a_tile(s, ar_a[q]) + k8 * 32),
+                      umma_desc_sw64(b_tile(s, ar_b[q]) + k8 * 32), id_wide,
                       (first | q) ? 1u : 0u);
-            umma_tf32(t_im, umma_desc_sw64(a_tile(s, im_a[q]) + k8 * 32),
-                      umma_desc_sw64(b_tile(s, im_b[q]) + k8 * 32), id_pos, (first | q) ? 1u : 0u);
+#pragma unroll
+          for (int q = 0; q < 3; ++q) {
+            umma_tf32(t_re, umma_desc_sw64(a_tile(s, ai_a[q]) + k8 * 32),
+                      umma_desc_sw64(b_tile(s, ai_bi[q]) + k8 * 32), id_neg, 1u);
+            umma_tf32(t_im, umma_desc_sw64(a_tile(s, ai_a[q]) + k8 * 32),
+                      umma_desc_sw64(b_tile(s, ai_br[q]) + k8 * 32), id_pos, 1u);
           }
         }
         umma_commit(&empty[s]);  // frees the stage when these MMAs complete
