@@ -663,8 +663,9 @@ static int euler_factors(const euv_amp_desc* d) {
   if (!(e < 0.5)) return 0;
   // The product serves the mixed form only, whose TF32x3 products carry ~1e-6
   // relative error each: a truncation ||E||^(2^F) <= 1e-7 stays below that.
+  // the product of F factors is sum_{j < 2^F} E^j: truncation ||E||^(2^F)
   int f = 1;
-  double v = e;  // ||E||^(2^f)
+  double v = e * e;  // ||E||^(2^f)
   while (v > 1e-7 && f < 8) {
     v = v * v;
     ++f;
