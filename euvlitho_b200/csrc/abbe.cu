@@ -25,6 +25,10 @@ struct cx {
   R x, y;
 };
 template <typename R>
+__device__ __forceinline__ cx<R> operator+(cx<R> a, cx<R> b);
+template <typename R>
+__device__ __forceinline__ cx<R> operator*(cx<R> a, cx<R> b);
+template <typename R>
 __device__ __forceinline__ cx<R> operator+(cx<R> a, cx<R> b) { return {a.x + b.x, a.y + b.y}; }
 template <typename R>
 __device__ __forceinline__ cx<R> operator*(cx<R> a, cx<R> b) {
@@ -42,7 +46,30 @@ struct vec2<float> {
 };
 
 constexpr int AB_YS = 4;
+
 constexpr int AB_THREADS = 256;
+
+// f[b][c] += G[lx][b][c] w for the AB_YS x 3 values of G at one lx (16 B
+// aligned): FP32 reads them as float4 pairs, FP64 one double2 at a time
+__device__ __forceinline__ void stage_x_lx(const float2* gp, cx<float> (&f)[AB_YS][3],
+                                           cx<float> w) {
+  const float4* q = reinterpret_cast<const float4*>(gp);
+#pragma unroll
+  for (int k = 0; k < AB_YS * 3 / 2; ++k) {
+    const float4 v = q[k];
+    const int e0 = 2 * k, e1 = 2 * k + 1;
+    f[e0 / 3][e0 % 3] = f[e0 / 3][e0 % 3] + cx<float>{v.x, v.y} * w;
+    f[e1 / 3][e1 % 3] = f[e1 / 3][e1 % 3] + cx<float>{v.z, v.w} * w;
+  }
+}
+__device__ __forceinline__ void stage_x_lx(const double2* gp, cx<double> (&f)[AB_YS][3],
+                                           cx<double> w) {
+#pragma unroll
+  for (int e = 0; e < AB_YS * 3; ++e) {
+    const double2 v = gp[e];
+    f[e / 3][e % 3] = f[e / 3][e % 3] + cx<double>{v.x, v.y} * w;
+  }
+}
 constexpr int AB_XPT = 4;  // x values per thread: xdiv <= 1024
 
 struct AbbeParams {
@@ -64,8 +91,9 @@ __global__ void __launch_bounds__(AB_THREADS) abbe_kernel(AbbeParams p, const do
   using C = cx<R>;
   extern __shared__ __align__(16) unsigned char sm_raw[];
   V2* E = reinterpret_cast<V2*>(sm_raw);              // [ncut][3]
-  V2* G = E + (size_t)p.ncut * 3;                     // [YS][bx][3]
+  V2* G = E + (((size_t)p.ncut * 3 + 1) & ~(size_t)1);  // [bx][YS][3], 16 B aligned
   V2* twy = G + (size_t)AB_YS * p.bx * 3;             // [YS][by]
+  int* s_py = reinterpret_cast<int*>(twy + (size_t)AB_YS * p.by);  // [ncut] pupil m + lpy
   const int u = blockIdx.z;
   const int y0 = blockIdx.x * AB_YS;
   const int tid = threadIdx.x;
@@ -81,6 +109,7 @@ __global__ void __launch_bounds__(AB_THREADS) abbe_kernel(AbbeParams p, const do
     sincospi(2.0 * (double)q / (double)p.ydiv, &s, &c);
     twy[idx] = V2{(R)c, (R)s};
   }
+  for (int i = tid; i < p.ncut; i += AB_THREADS) s_py[i] = p.py[i] + p.lpy;
 
   double acc[AB_XPT][AB_YS];
 #pragma unroll
@@ -108,17 +137,18 @@ __global__ void __launch_bounds__(AB_THREADS) abbe_kernel(AbbeParams p, const do
       E[i * 3 + 2] = V2{(R)e2.x, (R)e2.y};
     }
     __syncthreads();
-    // stage y
+    // stage y; G[lx][yy][c]: the 3 AB_YS values stage x reads per lx are contiguous
     for (int o = tid; o < AB_YS * p.bx * 3; o += AB_THREADS) {
       const int c = o % 3, lx = (o / 3) % p.bx, yy = o / (3 * p.bx);
       C g{(R)0, (R)0};
       const int i0 = p.row_start[lx], i1 = p.row_start[lx + 1];
+      const V2* ty = twy + yy * p.by;
       for (int i = i0; i < i1; ++i) {
         const V2 e = E[i * 3 + c];
-        const V2 t = twy[yy * p.by + (p.py[i] + p.lpy)];
+        const V2 t = ty[s_py[i]];
         g = g + C{e.x, e.y} * C{t.x, t.y};
       }
-      G[o] = V2{g.x, g.y};
+      G[(lx * AB_YS + yy) * 3 + c] = V2{g.x, g.y};
     }
     __syncthreads();
     // stage x + |f|^2
@@ -136,15 +166,9 @@ __global__ void __launch_bounds__(AB_THREADS) abbe_kernel(AbbeParams p, const do
         C f[AB_YS][3];
 #pragma unroll
         for (int b = 0; b < AB_YS; ++b) f[b][0] = f[b][1] = f[b][2] = C{(R)0, (R)0};
-        for (int lx = 0; lx < p.bx; ++lx) {
-#pragma unroll
-          for (int b = 0; b < AB_YS; ++b) {
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-              const V2 g = G[(b * p.bx + lx) * 3 + c];
-              f[b][c] = f[b][c] + C{g.x, g.y} * w;
-            }
-          }
+        const V2* gp = G;
+        for (int lx = 0; lx < p.bx; ++lx, gp += AB_YS * 3) {
+          stage_x_lx(gp, f, w);
           w = w * r;
         }
 #pragma unroll
@@ -206,8 +230,9 @@ extern "C" int euv_abbe(const euv_abbe_desc* d, const euv_c64* d_ax, double* d_i
   if (nsplit > d->n_src) nsplit = d->n_src;
   p.nsplit = nsplit;
   const bool fp32 = d->precision == EUV_PREC_MIXED;
-  size_t smem = ((size_t)d->ncut * 3 + (size_t)AB_YS * p.bx * 3 + (size_t)AB_YS * p.by) *
-                (fp32 ? sizeof(float2) : sizeof(double2));
+  size_t smem = ((((size_t)d->ncut * 3 + 1) & ~(size_t)1) + (size_t)AB_YS * p.bx * 3 +
+                 (size_t)AB_YS * p.by) * (fp32 ? sizeof(float2) : sizeof(double2)) +
+                 (size_t)d->ncut * sizeof(int);
   if (smem > 227 * 1024) {
     euv_set_error("euv_abbe: pupil too large for one CTA (%zu bytes of shared memory)", smem);
     return EUV_ERR_BAD_ARG;
