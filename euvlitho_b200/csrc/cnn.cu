@@ -764,13 +764,7 @@ static size_t cnn_smem(int bn, int stages) {
 template <class Kern, class Args>
 static int cnn_launch(Kern kernel, dim3 grid, size_t smem, const CUtensorMap& ta,
                       const CUtensorMap& tb, const Args& p, cudaStream_t stream, int* done) {
-  int dev = 0;
-  EUV_CUDA_TRY(cudaGetDevice(&dev));
-  if (dev < 64 && done[dev] < (int)smem) {
-    EUV_CUDA_TRY(
-        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    done[dev] = (int)smem;
-  }
+  EUV_CUDA_TRY(ensure_smem(kernel, (int)smem, done));
   kernel<<<grid, CNN_THREADS, smem, stream>>>(ta, tb, p);
   EUV_LAUNCH_CHECK();
   return EUV_OK;
@@ -783,14 +777,10 @@ static int cnn_conv_grid(int total, int tmem_cols, size_t smem) {
   static int done[64];
   int dev = 0, nsm = 148, sm_smem = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return -1;
-  if (dev < 64 && done[dev] < (int)smem) {
-    if (cudaFuncSetAttribute(cnn_conv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem) != cudaSuccess ||
-        cudaFuncSetAttribute(cnn_conv_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
-                             (int)cudaSharedmemCarveoutMaxShared) != cudaSuccess)
-      return -1;
-    done[dev] = (int)smem;
-  }
+  if (ensure_smem(cnn_conv_kernel, (int)smem, done) != cudaSuccess ||
+      cudaFuncSetAttribute(cnn_conv_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                           (int)cudaSharedmemCarveoutMaxShared) != cudaSuccess)
+    return -1;
   cudaFuncAttributes fa;
   if (cudaFuncGetAttributes(&fa, cnn_conv_kernel) != cudaSuccess ||
       cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
