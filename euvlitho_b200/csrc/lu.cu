@@ -143,7 +143,6 @@ __global__ void __launch_bounds__(LP_THREADS) lu_panel_reg_kernel(int n, int j0,
   ipiv += (long long)blockIdx.x * n;
   __shared__ double red_v[LP_THREADS / 32];
   __shared__ int red_i[LP_THREADS / 32];
-  __shared__ int s_piv;
   __shared__ cplx s_rowa[LP_SB], s_prow[LP_SB];
   __shared__ cplx s_u12[LP_SB][LU_NB];
   __shared__ cplx s_l11[LP_SB][LP_SB];
@@ -190,27 +189,27 @@ __global__ void __launch_bounds__(LP_THREADS) lu_panel_reg_kernel(int n, int j0,
         red_i[warp] = bidx;
       }
       __syncthreads();
-      if (warp == 0) {  // the warp maxima, same rule (first index of the maximum)
+      // every warp reduces the warp maxima itself (same rule: first index of
+      // the maximum), so the pivot needs no second barrier
+      int piv;
+      {
         double bv = lane < LP_THREADS / 32 ? red_v[lane] : -1.0;
         int bi = lane < LP_THREADS / 32 ? red_i[lane] : n;
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) {
-          const double ov = __shfl_down_sync(0xffffffffu, bv, off);
-          const int oi = __shfl_down_sync(0xffffffffu, bi, off);
+          const double ov = __shfl_xor_sync(0xffffffffu, bv, off);
+          const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
           if (ov > bv || (ov == bv && oi < bi)) {
             bv = ov;
             bi = oi;
           }
         }
-        if (lane == 0) {
-          if (bi >= n) bi = jj;
-          s_piv = bi;
-          s_pivs[c] = bi;
-          ipiv[jj] = bi;
+        piv = bi >= n ? jj : bi;
+        if (tid == 0) {
+          s_pivs[c] = piv;
+          ipiv[jj] = piv;
         }
       }
-      __syncthreads();
-      const int piv = s_piv;
       // one exchange through shared memory: the new row jj (= old row piv) is
       // also the pivot row the update below broadcasts
 #pragma unroll
