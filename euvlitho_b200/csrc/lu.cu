@@ -424,6 +424,47 @@ __global__ void lu_trsm_block_kernel(int jb, int ncols, int lower, const double2
     if (r < jb) st2(&X[r + (long long)col * ldx], x[r]);
 }
 
+// The same solve with one warp per column: lane r holds row r of X; step q
+// broadcasts the finished x_q by shuffle and every later (lower) or earlier
+// (upper) lane subtracts its term, so a column takes jb short steps instead of
+// one thread's chain of jb^2/2 dependent products.  8 columns per CTA.
+constexpr int LU_TRSM_WARPS = 8;
+__global__ void __launch_bounds__(32 * LU_TRSM_WARPS)
+    lu_trsm_warp_kernel(int jb, int ncols, int lower, const double2* T, long long ldt,
+                        long long st, double2* X, long long ldx, long long sx) {
+  __shared__ double2 Ts[LU_NB][LU_NB + 1];
+  const int b = blockIdx.y;
+  T += (long long)b * st;
+  X += (long long)b * sx;
+  for (int idx = threadIdx.x; idx < jb * jb; idx += blockDim.x) {
+    const int r = idx % jb, c = idx / jb;
+    Ts[r][c] = T[r + (long long)c * ldt];
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int col = blockIdx.x * LU_TRSM_WARPS + (threadIdx.x >> 5);
+  if (col >= ncols) return;  // whole warps: col is warp-uniform
+  double2* Xc = X + (long long)col * ldx;
+  cplx x = lane < jb ? ld2(&Xc[lane]) : mk(0.0, 0.0);
+  if (lower) {
+    for (int q = 0; q < jb; ++q) {
+      const cplx xq = mk(__shfl_sync(0xffffffffu, x.x, q), __shfl_sync(0xffffffffu, x.y, q));
+      if (lane > q && lane < jb) x = x - mk(Ts[lane][q].x, Ts[lane][q].y) * xq;
+    }
+  } else {
+    for (int q = jb - 1; q >= 0; --q) {
+      if (lane == q) x = cdiv(x, mk(Ts[q][q].x, Ts[q][q].y));
+      const cplx xq = mk(__shfl_sync(0xffffffffu, x.x, q), __shfl_sync(0xffffffffu, x.y, q));
+      if (lane < q) x = x - mk(Ts[lane][q].x, Ts[lane][q].y) * xq;
+    }
+  }
+  if (lane < jb) st2(&Xc[lane], x);
+}
+
+static inline dim3 trsm_grid(int ncols, int batch) {
+  return dim3((ncols + LU_TRSM_WARPS - 1) / LU_TRSM_WARPS, batch);
+}
+
 __global__ void zero_int_kernel(int* p, int n) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) p[i] = 0;
@@ -473,9 +514,8 @@ static int lu_panel(int n, int j0, int jb, double2* A, long long lda, long long 
 static int lu_update(int n, int j0, int jb, int c0, int nc, double2* A, long long lda,
                      long long sa, int batch, cudaStream_t st) {
   if (nc <= 0) return EUV_OK;
-  dim3 gt((nc + 127) / 128, batch);
-  lu_trsm_block_kernel<<<gt, 128, 0, st>>>(jb, nc, 1, A + j0 + (long long)j0 * lda, lda, sa,
-                                           A + j0 + (long long)c0 * lda, lda, sa);
+  lu_trsm_warp_kernel<<<trsm_grid(nc, batch), 32 * LU_TRSM_WARPS, 0, st>>>(
+      jb, nc, 1, A + j0 + (long long)j0 * lda, lda, sa, A + j0 + (long long)c0 * lda, lda, sa);
   EUV_LAUNCH_CHECK();
   const int rest = n - j0 - jb;
   return zgemm_sub(rest, nc, jb, A + (j0 + jb) + (long long)j0 * lda, lda, sa,
