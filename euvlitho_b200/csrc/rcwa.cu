@@ -154,6 +154,29 @@ __global__ void __launch_bounds__(SC_THREADS) spectrum_cols_kernel(int fx, int l
   }
 }
 
+// Stage 2 as a split-K DMMA GEMM (out = Wx T^T, K = x in `parts` chunks, one
+// batch entry per chunk): the chunk partial sums, added here.
+__global__ void spectrum_reduce_kernel(const double2* part, int parts, long long total,
+                                       double2* out) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= total) return;
+  double2 s = part[t];
+  for (int p = 1; p < parts; ++p) {
+    const double2 v = part[(long long)p * total + t];
+    s.x += v.x;
+    s.y += v.y;
+  }
+  out[t] = s;
+}
+
+// K chunks of stage 2 (0: the per-column kernel): fx / parts a multiple of 64
+static int spectrum_parts(int fx) {
+  if (fx % 64) return 0;
+  int parts = fx / 64 < 16 ? fx / 64 : 16;
+  while ((fx / 64) % parts) --parts;
+  return parts;
+}
+
 // W[r + rows*c] = scale * exp(-2 pi i ((f*g) mod fdiv)/fdiv) with f = r - roff
 // (frequency) and g = c - coff (sample), or transposed roles when `freq_rows`==0.
 __global__ void twiddle_kernel(int rows, int cols, int roff, int coff, int fdiv, int freq_rows,
@@ -983,7 +1006,10 @@ extern "C" size_t euv_mask_spectrum_workspace_bytes(int n_masks, int ndivx, int 
   Bump bp{nullptr, (size_t)-1, 0, true};
   bp.take<double2>((size_t)fdivy * mr);
   bp.take<double2>(lr * (size_t)fdivx);
-  bp.take<double2>((size_t)(n_masks > 1 ? n_masks : 1) * mr * fdivx);
+  const size_t nm = n_masks > 1 ? n_masks : 1;
+  bp.take<double2>(nm * mr * fdivx);
+  bp.take<double2>(nm * (size_t)spectrum_parts(fdivx) * lr * mr);
+  bp.take<char>(256);  // the run's alignment slack between the two arrays
   return bp.off;
 }
 
@@ -1004,9 +1030,11 @@ extern "C" int euv_mask_spectrum(const uint8_t* d_bits, int n_masks, int ndivx, 
   Bump bp{reinterpret_cast<char*>(d_work), work_bytes, 0, true};
   double2* Wy = bp.take<double2>((size_t)fdivy * mr);
   double2* Wx = bp.take<double2>((size_t)lr * fdivx);
-  const size_t per_mask = ((size_t)mr * fdivx * sizeof(double2) + 255) & ~(size_t)255;
-  const size_t left = bp.ok && work_bytes > bp.off ? work_bytes - bp.off : 0;
-  long long group = (long long)(left / per_mask);
+  const int parts = spectrum_parts(fdivx);
+  const size_t t_bytes = (size_t)mr * fdivx * sizeof(double2);
+  const size_t p_bytes = (size_t)parts * lr * mr * sizeof(double2);
+  const size_t left = bp.ok && work_bytes > bp.off + 256 ? work_bytes - bp.off - 256 : 0;
+  long long group = (long long)(left / (t_bytes + p_bytes));
   if (group > 65535) group = 65535;  // grid z / y limit
   if (!d_work || !bp.ok || group < 1) {
     euv_set_error("euv_mask_spectrum: workspace too small");
@@ -1028,8 +1056,22 @@ extern "C" int euv_mask_spectrum(const uint8_t* d_bits, int n_masks, int ndivx, 
                                                   ndivy, fdivx, fdivy, mr, select_vacuum,
                                                   y_offset, Wy, T);
     EUV_LAUNCH_CHECK();
-    spectrum_cols_kernel<<<dim3(mr, ng), SC_THREADS, 0, stream>>>(
-        fdivx, lr, mr, Wx, T, reinterpret_cast<double2*>(d_out) + g0 * lr * mr);
+    double2* out = reinterpret_cast<double2*>(d_out) + g0 * lr * mr;
+    if (parts > 0) {
+      // out (lr x ng mr) = Wx (lr x FX) T^T (FX x ng mr), K split in `parts` chunks
+      const int kc = fdivx / parts;
+      const long long cols = (long long)ng * mr;
+      double2* P = reinterpret_cast<double2*>(
+          reinterpret_cast<char*>(T) + ((ng * t_bytes + 255) & ~(size_t)255));
+      int rc = zgemm(lr, (int)cols, kc, mk(1.0, 0.0), nullptr, Wx, lr, (long long)kc * lr, T,
+                     fdivx, kc, mk(0.0, 0.0), P, lr, (long long)lr * cols, mk(0.0, 0.0), parts,
+                     nullptr, 0, stream);
+      if (rc) return rc;
+      const long long total = (long long)lr * cols;
+      spectrum_reduce_kernel<<<grid1(total, 256), 256, 0, stream>>>(P, parts, total, out);
+    } else {
+      spectrum_cols_kernel<<<dim3(mr, ng), SC_THREADS, 0, stream>>>(fdivx, lr, mr, Wx, T, out);
+    }
     EUV_LAUNCH_CHECK();
   }
   return EUV_OK;

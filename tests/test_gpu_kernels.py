@@ -128,7 +128,8 @@ def test_matfun_cos_sinc(cuda, n, d):
     assert rel_err(_from_colmajor(ds.cpu().numpy(), n, n)[0], sref) < 1e-11
 
 
-@pytest.mark.parametrize("P,delta,lh,mh,vac", [(64, 1.0, 6, 6, 0), (64, 0.5, 4, 7, 1), (256, 1.0, 10, 10, 0)])
+@pytest.mark.parametrize("P,delta,lh,mh,vac", [(64, 1.0, 6, 6, 0), (64, 0.5, 4, 7, 1), (256, 1.0, 10, 10, 0),
+                                               (96, 1.0, 5, 5, 0)])
 def test_mask_spectrum(cuda, P, delta, lh, mh, vac):
     import torch
     from tests.helpers import packed
@@ -149,6 +150,30 @@ def test_mask_spectrum(cuda, P, delta, lh, mh, vac):
     torch.cuda.synchronize()
     got = out.cpu().numpy().reshape(2 * mh + 1, 2 * lh + 1).T
     assert np.max(np.abs(got - ref)) < 1e-14
+
+
+def test_mask_spectrum_batch(cuda):
+    """Three 1024^2 masks in one call (the second stage's K split in 16 chunks
+    over all masks' columns) against per-mask FFTs."""
+    import torch
+    from tests.helpers import packed
+    P, lh, mh = 1024, 15, 12
+    masks = [random_mask(P, P, seed=40 + i) for i in range(3)]
+    cfg = O.SimConfig(ndivx=P, ndivy=P, delta=1.0)
+    bits = _t(np.stack([packed(m) for m in masks]), cuda)
+    lr, mr = 2 * lh + 1, 2 * mh + 1
+    out = torch.empty((3, lr * mr), dtype=torch.complex128, device=cuda)
+    wb = L.lib().euv_mask_spectrum_workspace_bytes(3, P, P, P, P, lh, mh)
+    ws = torch.empty(wb, dtype=torch.uint8, device=cuda)
+    L.call("euv_mask_spectrum", bits.data_ptr(), 3, P, P, P, P, lh, mh, 0, 0, out.data_ptr(),
+           ws.data_ptr(), wb, _stream())
+    torch.cuda.synchronize()
+    for i, m in enumerate(masks):
+        pat = O.mask_pattern(flat_bits(m), cfg, 1.0, 0.0)
+        F = np.fft.fft2(pat) / pat.size
+        ref = F[np.ix_(np.arange(-lh, lh + 1) % P, np.arange(-mh, mh + 1) % P)]
+        got = out[i].cpu().numpy().reshape(mr, lr).T
+        assert np.max(np.abs(got - ref)) < 1e-14, i
 
 
 @pytest.mark.parametrize("m,n,k,batch", [(128, 256, 16, 1), (121, 121, 121, 2), (300, 200, 77, 2), (961, 961, 961, 2)])
