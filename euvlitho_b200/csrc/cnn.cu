@@ -599,7 +599,7 @@ __global__ void __launch_bounds__(CNN_THREADS) cnn_fc_kernel(
   if (threadIdx.x == 0) {
     for (int s = 0; s < p.stages; ++s) {
       mbar_init(&full[s], 1);
-      mbar_init(&conv[s], 4);
+      mbar_init(&conv[s], 2);
       mbar_init(&empty[s], 1);
     }
     mbar_init(accum, 1);
@@ -647,9 +647,11 @@ __global__ void __launch_bounds__(CNN_THREADS) cnn_fc_kernel(
       umma_commit(accum);
     }
   } else {
-    // weight split: 2048 fp32 of the stage's A tile, 16 per thread
-    const int et = threadIdx.x - 64;  // 0..127
-    for (int kb = 0; kb < nkb; ++kb) {
+    // weight split, 2048 fp32 of a stage's A tile: warps 2-3 take the even K
+    // blocks, warps 4-5 the odd ones (two stages converting at once), 32 per thread
+    const int grp = (warp - 2) >> 1;
+    const int et = threadIdx.x - 64 - 64 * grp;  // 0..63
+    for (int kb = grp; kb < nkb; kb += 2) {
       const int s = kb % p.stages;
       const uint32_t ph = (uint32_t)((kb / p.stages) & 1);
       const bool got = mbar_wait_bounded(&full[s], ph, abort_flag, p.err, CNN_TIMEOUT_NS);
@@ -657,8 +659,8 @@ __global__ void __launch_bounds__(CNN_THREADS) cnn_fc_kernel(
       float4* hi = reinterpret_cast<float4*>(ring.a(s, 0));
       float4* lo = reinterpret_cast<float4*>(ring.a(s, 1));
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int i = et + 128 * u;
+      for (int u = 0; u < 8; ++u) {
+        const int i = et + 64 * u;
         const float4 x = hi[i];
         float4 h, l;
         split_tf32f(x.x, h.x, l.x);
