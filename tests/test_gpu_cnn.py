@@ -101,3 +101,31 @@ def test_predict_rejects_a_bad_batch(predictor):
         predictor.as_bits(torch.zeros((1, cnn.MASK_BYTES), dtype=torch.float32))
     with pytest.raises(ValueError):
         predictor.workspace(0)
+
+
+def test_predict_more_masks_than_one_tile(cuda, models):
+    """260 masks (two 256-mask tiles of the fc layers, the second holding 4):
+    one network, 10 distinct rasters repeated; every repeat matches its first
+    occurrence (to 1e-6) and a sample of them the FP32 oracle."""
+    facs = O.seeded_factors()
+    pred = cnn.CnnPredictor(O.state_dicts(models[:1]), [facs[0]], cuda)
+    base = rasters(10, 11)
+    raw = np.concatenate([base] * 26)
+    got = pred.predict(raw)[0]
+    assert got.shape == (260, O.NCUT)
+    for i in range(10, 260):
+        assert _rel(got[i], got[i % 10]) < 1e-6, i
+    x = torch.from_numpy(np.stack([O.compmask_bits(r) for r in base])).reshape(-1, 1, 512, 512)
+    prev = (torch.backends.cuda.matmul.allow_tf32, torch.backends.cudnn.allow_tf32)
+    torch.backends.cuda.matmul.allow_tf32 = False
+    torch.backends.cudnn.allow_tf32 = False
+    try:
+        m = models[0].to(cuda)
+        with torch.no_grad():
+            ref = m(x.to(cuda)).double().cpu().numpy() / facs[0]
+        models[0].to("cpu")
+    finally:
+        torch.backends.cuda.matmul.allow_tf32, torch.backends.cudnn.allow_tf32 = prev
+    for i in (0, 7, 256, 259):
+        err = _rel(got[i], ref[i % 10])
+        assert err < TOL, (i, err)
