@@ -139,3 +139,58 @@ def test_mixed_precision_intensity_within_1e4(cuda, name):
         ref = O.intensity(oc, flat_bits(m), polars=("X", "Y"))
         for p, pol in enumerate(("X", "Y")):
             assert rel_err(img[c, p], ref[pol]) < 1e-4
+
+
+# Mixed form, outputs other than the image: the amplitudes and the M3D
+# parameters against the FP64 oracle, max |x - x_ref| / max |x_ref| per array.
+MIXED_AMP_TOL = 1e-4
+
+
+@pytest.mark.parametrize("name", ["small", "mixed"])
+def test_mixed_precision_amplitudes(cuda, name):
+    import torch
+    from euvlitho_b200.engine import Plan
+    cfg = preset(name)
+    oc = to_oracle(cfg)
+    plan = Plan(cfg, device=cuda, pols=("X",), precision="mixed")
+    ms = _masks(cfg, [41, 42])
+    ax, srcs = plan.amp(torch.from_numpy(np.stack([packed(m) for m in ms])), polar="X")
+    ax = ax.cpu().numpy()
+    L, M = cfg.order_limits()
+    worst = 0.0
+    for c, m in enumerate(ms):
+        ref = O.amp_s("X", flat_bits(m), oc, plan.orders.lidx, plan.orders.midx, L, M, oc.kx0, oc.ky0)
+        for s, key in enumerate(srcs):
+            worst = max(worst, rel_err(ax[c, s], ref[key]))
+    print("mixed amplitudes %s: max rel err %.2e" % (name, worst))
+    assert worst < MIXED_AMP_TOL
+
+
+# M3D parameters of the mixed form: ax, ay are least-squares slopes over the
+# sources that see a pupil order, and a slope can vanish (ax is ~1e-15 on this
+# clip: no x tilt of the chief ray), so every parameter's error is measured
+# against the scale of a0; the fit amplifies amplitude errors about 5-10x
+# (1e-5 noise on the oracle's amplitudes gives 5e-5 on a0, 1e-4 on ay), yet
+# the mixed form stays within the image's 1e-4 bar here.
+MIXED_M3D_TOL = 1e-4
+
+
+def test_mixed_precision_m3d_parameters(cuda):
+    import torch
+    from euvlitho_b200.engine import Plan
+    cfg = SimConfig(ndivx=512, ndivy=512)
+    oc = to_oracle(cfg)
+    plan = Plan(cfg, device=cuda, pols=("X",), precision="mixed")
+    m = random_mask(512, 512, seed=43)
+    res = plan.m3d(torch.from_numpy(packed(m)[None]))
+    ref = O.m3d(oc, flat_bits(m))
+    xin = plan.xinput == 1
+    scale = np.max(np.abs(ref["a0"]))
+    errs = {"a0": np.max(np.abs(res["a0"][0].cpu().numpy() - ref["a0"])) / scale}
+    if xin.any():
+        for k in ("ax", "ay"):
+            errs[k] = np.max(np.abs(res[k][0].cpu().numpy()[xin] - ref[k])) / scale
+    print("mixed M3D parameters (max abs err / max |a0|): " +
+          ", ".join("%s %.2e" % kv for kv in errs.items()))
+    for k, e in errs.items():
+        assert e < MIXED_M3D_TOL, (k, e)
