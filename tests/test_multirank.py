@@ -33,7 +33,7 @@ def _worker(rank, world, port, out):
 
 def test_two_rank_replicas_gloo():
     world = 2
-    mgr = mp.Manager()
+    mgr = mp.get_context("spawn").Manager()
     out = mgr.dict()
     mp.spawn(_worker, args=(world, _free_port(), out), nprocs=world, join=True)
     assert out[0][0] == out[1][0] == 150.0                    # max over ranks
