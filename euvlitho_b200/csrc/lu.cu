@@ -6,9 +6,9 @@
 // the right-hand sides it needs.
 //
 // Blocked right-looking LU, panel width LU_NB:
-//   panel  : one CTA per matrix factors columns [j0, j0+nb) of rows [j0, n)
-//            (pivot = first max of |re|+|im| as LAPACK izamax, row swap inside
-//            the panel, scale, rank-1 update), sub-panels in registers;
+//   panel  : columns [j0, j0+nb) of rows [j0, n) (pivot = first max of
+//            |re|+|im| as LAPACK izamax, row swap, scale, rank-1 update), the
+//            rows in the registers of a cluster of up to 8 CTAs per matrix;
 //   laswp  : the panel's row swaps applied to the other columns;
 //   trsm   : U12 = L11^-1 A12 (unit lower, L11 staged in shared memory);
 //   update : A22 -= L21 U12 with the batched DMMA zgemm;
@@ -16,9 +16,13 @@
 //            the rest of the update runs (the panel alone fills only `batch` SMs).
 // Solve: the row swaps on B, then one launch that keeps 8 (or fewer, for large
 // n) columns of X in shared memory per CTA through both substitutions.
+#include <cooperative_groups.h>
+
 #include "common.cuh"
 
 namespace euv {
+
+namespace cg = cooperative_groups;
 
 int zgemm_sub(int m, int n, int k, const double2* a, long long lda, long long sa,
               const double2* b, long long ldb, long long sb, double2* c, long long ldc,
@@ -122,228 +126,169 @@ __global__ void __launch_bounds__(LU_PANEL_THREADS) lu_panel_kernel(int n, int j
   }
 }
 
-// Panel factorisation with register-resident sub-panels (N <= 512*RPT): the
-// panel is factored LP_SB columns at a time; thread t holds rows
-// r0 + t + k*LP_THREADS (k < RPT) of the sub-panel in registers, so pivot
-// search, row exchange, scaling and the rank-1 updates inside the sub-panel
-// touch no global memory.  After each sub-panel, the rest of the panel is
-// brought up to date at once: its row swaps and U12 = L11^-1 A12 by one thread
-// per column (rows gathered into registers, L11 from shared memory), then
-// A22 -= L21 U12 with batched loads.  The panel's columns left of a sub-panel
-// get its swaps from the laswp launch that follows the panel (sub = LP_SB).
-constexpr int LP_THREADS = 512;
-constexpr int LP_SB = 4;
+// Panel factorisation by a cluster of LC CTAs per matrix with the panel rows
+// in registers (n - j0 <= LC * LC_THREADS rows): thread t of cluster rank q
+// holds row j0 + q*LC_THREADS + t.  Columns are taken in blocks of LC_BLK
+// with the block's columns at compile-time register indices v[0..LC_BLK); the
+// register row is rotated by LC_BLK after each block (one block's code for the
+// whole panel, no runtime register indexing).  One cluster barrier per column
+// jj: before it, every CTA finds its candidate (first max of |re|+|im| in its
+// rows >= jj, as izamax; every warp reduces the warp maxima itself) and sends
+// the candidate's value, index and row to every CTA through distributed shared
+// memory, one column per lane of the warp that holds the row, and rank 0 sends
+// row jj the same way; after it, every thread reduces the LC candidates in
+// rank order (same pivot in every CTA), takes the pivot row from the winner's
+// slot, swaps, scales and applies the rank-1 update to its own row.  Slots
+// alternate by column parity: a slot is rewritten two barriers after it was
+// read.  A block's columns are stored when it ends (final apart from later row
+// swaps), pivots and the singular flag when the panel ends.  Columns of rows
+// swapped by later pivots, and the columns left of the block of rows swapped
+// inside it, are fixed by the laswp launch after the panel (sub = 1: column c
+// gets the swaps of pivots c+1..).  Every thread executes every barrier the
+// same number of times whatever the data (a zero pivot skips only the
+// arithmetic).
+constexpr int LC_THREADS = 256;
+constexpr int LC_WARPS = LC_THREADS / 32;
+constexpr int LC_BLK = 4;
+static_assert(LU_NB == 32, "one panel column per lane");
+static_assert(LU_NB % LC_BLK == 0, "whole blocks");
 
-template <int RPT>
-__global__ void __launch_bounds__(LP_THREADS) lu_panel_reg_kernel(int n, int j0, int jb,
-                                                                  double2* A, long long lda,
-                                                                  long long sa, int* ipiv,
-                                                                  int* info) {
-  A += (long long)blockIdx.x * sa;
-  ipiv += (long long)blockIdx.x * n;
-  __shared__ double red_v[LP_THREADS / 32];
-  __shared__ int red_i[LP_THREADS / 32];
-  __shared__ cplx s_rowa[LP_SB], s_prow[LP_SB];
-  __shared__ cplx s_u12[LP_SB][LU_NB];
-  __shared__ cplx s_l11[LP_SB][LP_SB];
-  __shared__ int s_pivs[LP_SB];
+__device__ __forceinline__ void argmax_step(double& v, int& i, double ov, int oi) {
+  if (ov > v || (ov == v && oi < i)) {
+    v = ov;
+    i = oi;
+  }
+}
+
+template <int LC>
+__global__ void __cluster_dims__(LC, 1, 1) __launch_bounds__(LC_THREADS, 1)
+    lu_panel_cluster_kernel(int n, int j0, int jb, double2* A, long long lda, long long sa,
+                            int* ipiv, int* info) {
+  cg::cluster_group cluster = cg::this_cluster();
+  const int q = (int)cluster.block_rank();
+  const int mat = blockIdx.x / LC;
+  A += (long long)mat * sa;
+  ipiv += (long long)mat * n;
+  __shared__ double s_wv[LU_NB][LC_WARPS];
+  __shared__ int s_wi[LU_NB][LC_WARPS];
+  __shared__ double s_cv[LU_NB][LC];
+  __shared__ int s_ci[LU_NB][LC];
+  __shared__ double2 s_crow[2][LC][LU_NB];  // candidate rows, by rank
+  __shared__ double2 s_rjj[2][LU_NB];       // row jj
+  __shared__ int s_piv[LU_NB];
+  int zero_col = 0;  // first zero pivot + 1
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  for (int sub = 0; sub < jb; sub += LP_SB) {
-    const int sb = (jb - sub) < LP_SB ? (jb - sub) : LP_SB;
-    const int c0 = j0 + sub;
-    cplx v[RPT][LP_SB];
+  const int r = j0 + q * LC_THREADS + tid;
+  const bool own = r < n;
+  cplx v[LU_NB];
 #pragma unroll
-    for (int k = 0; k < RPT; ++k) {
-      const int r = c0 + tid + k * LP_THREADS;
+  for (int k = 0; k < LU_NB; ++k)
+    v[k] = (own && k < jb) ? ld2(&A[r + (long long)(j0 + k) * lda]) : mk(0.0, 0.0);
+#pragma unroll 1
+  for (int c0 = 0; c0 < jb; c0 += LC_BLK) {  // jb is the same for every thread
 #pragma unroll
-      for (int c = 0; c < LP_SB; ++c)
-        v[k][c] = (r < n && c < sb) ? ld2(&A[r + (long long)(c0 + c) * lda]) : mk(0.0, 0.0);
-    }
-    for (int c = 0; c < sb; ++c) {
-      const int jj = c0 + c;
-      // pivot: first index of max |re|+|im| in rows jj..n-1 (LAPACK izamax)
-      double best = -1.0;
-      int bidx = n;
+    for (int i = 0; i < LC_BLK; ++i) {
+      const int c = c0 + i;
+      if (c >= jb) break;
+      const int jj = j0 + c, buf = c & 1;
+      double best = (own && r >= jj) ? cabs1(v[i]) : -1.0;
+      int bidx = (own && r >= jj) ? r : n;
 #pragma unroll
-      for (int k = 0; k < RPT; ++k) {
-        const int r = c0 + tid + k * LP_THREADS;
-        if (r >= jj && r < n) {
-          const double a = cabs1(v[k][c]);
-          if (a > best) {
-            best = a;
-            bidx = r;
-          }
-        }
-      }
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) {
-        const double ov = __shfl_down_sync(0xffffffffu, best, off);
-        const int oi = __shfl_down_sync(0xffffffffu, bidx, off);
-        if (ov > best || (ov == best && oi < bidx)) {
-          best = ov;
-          bidx = oi;
-        }
-      }
+      for (int off = 16; off > 0; off >>= 1)
+        argmax_step(best, bidx, __shfl_xor_sync(0xffffffffu, best, off),
+                    __shfl_xor_sync(0xffffffffu, bidx, off));
       if (lane == 0) {
-        red_v[warp] = best;
-        red_i[warp] = bidx;
+        s_wv[c][warp] = best;
+        s_wi[c][warp] = bidx;
       }
       __syncthreads();
-      // every warp reduces the warp maxima itself (same rule: first index of
-      // the maximum), so the pivot needs no second barrier
-      int piv;
       {
-        double bv = lane < LP_THREADS / 32 ? red_v[lane] : -1.0;
-        int bi = lane < LP_THREADS / 32 ? red_i[lane] : n;
+        double bv = lane < LC_WARPS ? s_wv[c][lane] : -1.0;
+        int bi = lane < LC_WARPS ? s_wi[c][lane] : n;
 #pragma unroll
-        for (int off = 16; off > 0; off >>= 1) {
-          const double ov = __shfl_xor_sync(0xffffffffu, bv, off);
-          const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
-          if (ov > bv || (ov == bv && oi < bi)) {
-            bv = ov;
-            bi = oi;
+        for (int off = LC_WARPS / 2; off > 0; off >>= 1)
+          argmax_step(bv, bi, __shfl_xor_sync(0xffffffffu, bv, off),
+                      __shfl_xor_sync(0xffffffffu, bi, off));
+        // lane 0 decides (the lanes agree unless a NaN breaks the order)
+        bv = __shfl_sync(0xffffffffu, bv, 0);
+        bi = __shfl_sync(0xffffffffu, bi, 0);
+        if (bi < n && (bi - j0 - q * LC_THREADS) >> 5 == warp) {
+          if (r == bi)
+#pragma unroll
+            for (int k = i; k < LU_NB; ++k) s_crow[buf][q][k] = make_double2(v[k].x, v[k].y);
+          __syncwarp();
+          if (lane >= i) {
+            const double2 x = s_crow[buf][q][lane];
+#pragma unroll
+            for (int t = 0; t < LC; ++t)
+              if (t != q) *cluster.map_shared_rank(&s_crow[buf][q][lane], t) = x;
           }
         }
-        piv = bi >= n ? jj : bi;
-        if (tid == 0) {
-          s_pivs[c] = piv;
-          ipiv[jj] = piv;
+        if (warp == 0 && lane < LC) {
+          *cluster.map_shared_rank(&s_cv[c][q], lane) = bv;
+          *cluster.map_shared_rank(&s_ci[c][q], lane) = bi;
         }
       }
-      // one exchange through shared memory: the new row jj (= old row piv) is
-      // also the pivot row the update below broadcasts
+      if (q == 0 && warp == 0) {
+        if (lane == c)
 #pragma unroll
-      for (int k = 0; k < RPT; ++k) {
-        const int r = c0 + tid + k * LP_THREADS;
+          for (int k = i; k < LU_NB; ++k) s_rjj[buf][k] = make_double2(v[k].x, v[k].y);
+        __syncwarp();
+        if (lane >= i) {
+          const double2 x = s_rjj[buf][lane];
 #pragma unroll
-        for (int cc = 0; cc < LP_SB; ++cc) {
-          if (r == piv) s_prow[cc] = v[k][cc];
-          if (r == jj) s_rowa[cc] = v[k][cc];
+          for (int t = 1; t < LC; ++t) *cluster.map_shared_rank(&s_rjj[buf][lane], t) = x;
         }
       }
-      __syncthreads();
-      if (piv != jj) {
+      cluster.sync();
+      double bv = s_cv[c][0];
+      int bi = s_ci[c][0], qw = 0;
 #pragma unroll
-        for (int k = 0; k < RPT; ++k) {
-          const int r = c0 + tid + k * LP_THREADS;
-#pragma unroll
-          for (int cc = 0; cc < LP_SB; ++cc) {
-            if (r == jj) v[k][cc] = s_prow[cc];
-            if (r == piv) v[k][cc] = s_rowa[cc];
-          }
+      for (int t = 1; t < LC; ++t) {
+        const double ov = s_cv[c][t];
+        const int oi = s_ci[c][t];
+        if (ov > bv || (ov == bv && oi < bi)) {
+          bv = ov;
+          bi = oi;
+          qw = t;
         }
       }
-      const cplx d = s_prow[c];
-      if (d.x == 0.0 && d.y == 0.0) {
-        if (tid == 0 && info[blockIdx.x] == 0) info[blockIdx.x] = jj + 1;
-        continue;
+      const int piv = (bi < jj || bi >= n) ? jj : bi;
+      if (tid == 0) s_piv[c] = piv;
+      const double2* prow = piv == jj ? s_rjj[buf] : s_crow[buf][qw];
+      if (own && piv != jj && (r == jj || r == piv)) {
+        const double2* src = r == jj ? prow : s_rjj[buf];
+#pragma unroll
+        for (int k = i; k < LU_NB; ++k) v[k] = mk(src[k].x, src[k].y);
       }
-      const cplx inv = cdiv(mk(1.0, 0.0), d);
+      const double2 dd = prow[i];
+      if (dd.x == 0.0 && dd.y == 0.0) {
+        if (zero_col == 0) zero_col = jj + 1;
+      } else if (own && r > jj) {
+        const cplx l = v[i] * cdiv(mk(1.0, 0.0), mk(dd.x, dd.y));
+        v[i] = l;
+        // columns c+1 .. jb-1 are v[i+1 .. jb-1-c0]; blocks of 8 past them are skipped
 #pragma unroll
-      for (int k = 0; k < RPT; ++k) {
-        const int r = c0 + tid + k * LP_THREADS;
-        if (r > jj && r < n) {
-          v[k][c] = v[k][c] * inv;
+        for (int k0 = 0; k0 < LU_NB; k0 += 8) {
+          if (k0 + 8 > i + 1 && k0 < jb - c0) {
 #pragma unroll
-          for (int cc = 0; cc < LP_SB; ++cc)
-            if (cc > c && cc < sb) v[k][cc] = v[k][cc] - v[k][c] * s_prow[cc];
-        }
-      }
-    }
-#pragma unroll
-    for (int k = 0; k < RPT; ++k) {
-      const int r = c0 + tid + k * LP_THREADS;
-      if (r < n)
-#pragma unroll
-        for (int c = 0; c < LP_SB; ++c)
-          if (c < sb) st2(&A[r + (long long)(c0 + c) * lda], v[k][c]);
-      if (r < c0 + sb)  // the unit-lower diagonal block L11, for U12 below
-#pragma unroll
-        for (int c = 0; c < LP_SB; ++c) s_l11[r - c0][c] = v[k][c];
-    }
-    const int rest = j0 + jb - (c0 + sb);  // panel columns right of the sub-panel
-    if (rest > 0) {
-      __syncthreads();
-      // one thread per column to the right: the sub-panel's row swaps (the
-      // rows c0.. and the pivot rows gathered into registers, swapped, stored
-      // back), then U12 = L11^-1 A12 on the swapped values; the panel's columns
-      // to the left get these swaps from the laswp launch after the panel
-      if (tid < rest) {
-        const int col = c0 + sb + tid;
-        double2* Ac = A + (long long)col * lda;
-        int rows[2 * LP_SB];
-        cplx val[2 * LP_SB];
-        int nr = 0;
-#pragma unroll
-        for (int i = 0; i < LP_SB; ++i)
-          if (i < sb) rows[nr++] = c0 + i;
-#pragma unroll
-        for (int c = 0; c < LP_SB; ++c) {
-          if (c < sb) {
-            const int pr = s_pivs[c];
-            bool seen = false;
-            for (int t = 0; t < nr; ++t) seen |= (rows[t] == pr);
-            if (!seen) rows[nr++] = pr;
-          }
-        }
-        for (int t = 0; t < nr; ++t) val[t] = ld2(&Ac[rows[t]]);
-#pragma unroll
-        for (int c = 0; c < LP_SB; ++c) {
-          if (c < sb) {
-            const int pr = s_pivs[c];
-            if (pr != c0 + c) {
-              int ia = 0, ib = 0;
-              for (int t = 0; t < nr; ++t) {
-                if (rows[t] == c0 + c) ia = t;
-                if (rows[t] == pr) ib = t;
-              }
-              const cplx x = val[ia];
-              val[ia] = val[ib];
-              val[ib] = x;
-            }
-          }
-        }
-        // rows c0..c0+sb-1 are val[0..sb-1]: forward substitution with L11
-#pragma unroll
-        for (int i = 0; i < LP_SB; ++i) {
-          if (i < sb) {
-            cplx u = val[i];
-#pragma unroll
-            for (int q = 0; q < LP_SB; ++q)
-              if (q < i) u = u - s_l11[i][q] * s_u12[q][tid];
-            s_u12[i][tid] = u;
-            val[i] = u;
-          }
-        }
-        for (int t = 0; t < nr; ++t) st2(&Ac[rows[t]], val[t]);
-      }
-      __syncthreads();
-      // A22 -= L21 U12 for rows below the sub-panel (L21 in registers), eight
-      // columns at a time with every load issued before the stores
-#pragma unroll
-      for (int k = 0; k < RPT; ++k) {
-        const int r = c0 + tid + k * LP_THREADS;
-        if (r >= c0 + sb && r < n) {
-          for (int j0b = 0; j0b < rest; j0b += 8) {
-            cplx a8[8];
-#pragma unroll
-            for (int j = 0; j < 8; ++j)
-              if (j0b + j < rest) a8[j] = ld2(&A[r + (long long)(c0 + sb + j0b + j) * lda]);
-#pragma unroll
-            for (int j = 0; j < 8; ++j) {
-              if (j0b + j < rest) {
-                cplx acc = a8[j];
-#pragma unroll
-                for (int q = 0; q < LP_SB; ++q)
-                  if (q < sb) acc = acc - v[k][q] * s_u12[q][j0b + j];
-                st2(&A[r + (long long)(c0 + sb + j0b + j) * lda], acc);
-              }
-            }
+            for (int k = k0; k < k0 + 8; ++k)
+              if (k > i) v[k] = v[k] - l * mk(prow[k].x, prow[k].y);
           }
         }
       }
     }
-    __syncthreads();
+    if (own)
+#pragma unroll
+      for (int i = 0; i < LC_BLK; ++i)
+        if (c0 + i < jb) st2(&A[r + (long long)(j0 + c0 + i) * lda], v[i]);
+#pragma unroll
+    for (int k = 0; k < LU_NB; ++k) v[k] = k + LC_BLK < LU_NB ? v[k + LC_BLK] : mk(0.0, 0.0);
+  }
+  __syncthreads();
+  if (q == 0) {
+    if (tid < jb) ipiv[j0 + tid] = s_piv[tid];
+    if (tid == 0 && zero_col != 0 && info[mat] == 0) info[mat] = zero_col;
   }
 }
 
@@ -495,14 +440,22 @@ static cudaError_t lu_side(LuSide** out) {
   return cudaSuccess;
 }
 
+// Row-swap granularity the laswp after panel j0 applies to the panel's own
+// columns: 1 after the cluster kernel (column c lacks the swaps of pivots
+// c+1..), 0 after lu_panel_kernel (the panel's columns are complete).
+static int panel_sub(int n, int j0) { return n - j0 <= 8 * LC_THREADS ? 1 : 0; }
+
 static int lu_panel(int n, int j0, int jb, double2* A, long long lda, long long sa, int* ipiv,
                     int* info, int batch, cudaStream_t st) {
-  if (n <= LP_THREADS)
-    lu_panel_reg_kernel<1><<<batch, LP_THREADS, 0, st>>>(n, j0, jb, A, lda, sa, ipiv, info);
-  else if (n <= 2 * LP_THREADS)
-    lu_panel_reg_kernel<2><<<batch, LP_THREADS, 0, st>>>(n, j0, jb, A, lda, sa, ipiv, info);
-  else if (n <= 4 * LP_THREADS)
-    lu_panel_reg_kernel<4><<<batch, LP_THREADS, 0, st>>>(n, j0, jb, A, lda, sa, ipiv, info);
+  const int rows = n - j0;
+  if (rows <= LC_THREADS)
+    lu_panel_cluster_kernel<1><<<batch, LC_THREADS, 0, st>>>(n, j0, jb, A, lda, sa, ipiv, info);
+  else if (rows <= 2 * LC_THREADS)
+    lu_panel_cluster_kernel<2><<<2 * batch, LC_THREADS, 0, st>>>(n, j0, jb, A, lda, sa, ipiv, info);
+  else if (rows <= 4 * LC_THREADS)
+    lu_panel_cluster_kernel<4><<<4 * batch, LC_THREADS, 0, st>>>(n, j0, jb, A, lda, sa, ipiv, info);
+  else if (rows <= 8 * LC_THREADS)
+    lu_panel_cluster_kernel<8><<<8 * batch, LC_THREADS, 0, st>>>(n, j0, jb, A, lda, sa, ipiv, info);
   else
     lu_panel_kernel<<<batch, LU_PANEL_THREADS, 0, st>>>(n, j0, jb, A, lda, sa, ipiv, info);
   EUV_LAUNCH_CHECK();
@@ -535,13 +488,12 @@ int lu_factor(int n, double2* A, long long lda, long long sa, int* ipiv, int* in
   EUV_CUDA_TRY(lu_side(&side));
   zero_int_kernel<<<(batch + 255) / 256, 256, 0, stream>>>(info, batch);
   EUV_LAUNCH_CHECK();
-  const int sub = n <= 4 * LP_THREADS ? LP_SB : 0;
   int j0 = 0, jb = n < LU_NB ? n : LU_NB;
   int rc = lu_panel(n, j0, jb, A, lda, sa, ipiv, info, batch, stream);
   if (rc) return rc;
   for (;;) {
     dim3 gs((n + 127) / 128, batch);
-    lu_laswp_kernel<<<gs, 128, 0, stream>>>(n, n, j0, jb, j0, j0 + jb, A, lda, sa, ipiv, n, sub);
+    lu_laswp_kernel<<<gs, 128, 0, stream>>>(n, n, j0, jb, j0, j0 + jb, A, lda, sa, ipiv, n, panel_sub(n, j0));
     EUV_LAUNCH_CHECK();
     const int rest = n - j0 - jb;
     if (rest <= 0) break;

@@ -70,7 +70,8 @@ def test_zgemm_step_copy(cuda):
     assert rel_err(got[2], A[2]) == 0.0
 
 
-@pytest.mark.parametrize("n,nrhs,batch", [(1, 1, 1), (31, 5, 2), (121, 121, 4), (200, 17, 2), (961, 40, 2)])
+@pytest.mark.parametrize("n,nrhs,batch", [(1, 1, 1), (31, 5, 2), (121, 121, 4), (200, 17, 2), (300, 9, 3),
+                                           (961, 40, 2), (1300, 8, 1), (1681, 16, 1)])
 def test_lu_solve(cuda, n, nrhs, batch):
     import torch
     rng = np.random.default_rng(n)
@@ -89,9 +90,9 @@ def test_lu_solve(cuda, n, nrhs, batch):
     assert rel_err(X, ref) < 1e-10
 
 
-def test_lu_reports_singular(cuda):
+@pytest.mark.parametrize("n", [40, 600])
+def test_lu_reports_singular(cuda, n):
     import torch
-    n = 40
     A = np.zeros((1, n, n), complex)
     A[0, :, :] = np.arange(n)[None, :]  # rank one
     dA = _t(_colmajor(A), cuda)
