@@ -56,6 +56,7 @@ struct MixedArgs {
   const double2* a;  // original FP64 A (copy mode)
   long long lda, sa;
   double2* c;
+  const double2* cin;  // C read by the beta term (c when null)
   long long ldc, sc;
   const int* steps;
   int step;
@@ -226,6 +227,7 @@ __global__ void __launch_bounds__(MX_THREADS, 1)
     const cplx alpha = mk(p.alpha.x * sc, p.alpha.y * sc);
     const cplx beta = mk(p.beta.x, p.beta.y);
     const bool use_beta = (p.beta.x != 0.0 || p.beta.y != 0.0);
+    const double2* Cin = p.cin ? p.cin + (long long)b * p.sc : C;
     const cplx dg = mk(p.diag.x, p.diag.y);
     if (ok) {
       for (int c0 = 0; c0 < MX_BN; c0 += 16) {
@@ -245,7 +247,7 @@ __global__ void __launch_bounds__(MX_THREADS, 1)
 #pragma unroll
             for (int j = 0; j < 16; ++j) {
               const int col = n0 + c0 + j;
-              old[j] = col < p.n ? C[row + (long long)col * p.ldc] : make_double2(0.0, 0.0);
+              old[j] = col < p.n ? Cin[row + (long long)col * p.ldc] : make_double2(0.0, 0.0);
             }
           }
 #pragma unroll
@@ -360,7 +362,7 @@ int gemm_mixed(int m, int n, int k, cplx alpha, const double* scale, const doubl
                long long lda, long long sa, const double2* b, long long ldb, long long sb,
                cplx beta, double2* c, long long ldc, long long sc, cplx diag, int batch,
                const int* steps, int step, void* work, size_t work_bytes, int* status,
-               cudaStream_t stream, int reuse) {
+               cudaStream_t stream, int reuse, const double2* cin) {
   if (m <= 0 || n <= 0 || batch <= 0) return EUV_OK;
   if (k <= 0 || batch > 65535 || (size_t)batch * MX_PLANES > 0x7fffffff) {
     euv_set_error("gemm_mixed: unsupported shape");
@@ -416,6 +418,7 @@ int gemm_mixed(int m, int n, int k, cplx alpha, const double* scale, const doubl
   p.lda = lda;
   p.sa = sa;
   p.c = c;
+  p.cin = cin;
   p.ldc = ldc;
   p.sc = sc;
   p.steps = steps;
@@ -450,5 +453,5 @@ extern "C" int euv_zgemm_tf32x3(int m, int n, int k, euv_c64 alpha, const double
   return gemm_mixed(m, n, k, fromc(alpha), d_scale, reinterpret_cast<const double2*>(d_a), lda,
                     stride_a, reinterpret_cast<const double2*>(d_b), ldb, stride_b, fromc(beta),
                     reinterpret_cast<double2*>(d_c), ldc, stride_c, fromc(diag), batch, d_steps,
-                    step, d_work, work_bytes, d_status, (cudaStream_t)stream, 0);
+                    step, d_work, work_bytes, d_status, (cudaStream_t)stream, 0, nullptr);
 }

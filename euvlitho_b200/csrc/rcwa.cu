@@ -38,7 +38,7 @@ int gemm_mixed(int m, int n, int k, cplx alpha, const double* scale, const doubl
                long long lda, long long sa, const double2* b, long long ldb, long long sb,
                cplx beta, double2* c, long long ldc, long long sc, cplx diag, int batch,
                const int* steps, int step, void* work, size_t work_bytes, int* status,
-               cudaStream_t stream, int reuse);
+               cudaStream_t stream, int reuse, const double2* cin);
 size_t gemm_mixed_workspace_bytes(int m, int n, int k, int batch);
 
 // ||A||_1 bound for the degree-8 Taylor step of cos/sin(sqrt(A)): the dropped
@@ -562,10 +562,16 @@ struct Gemm {
   int operator()(int m, int n, int k, cplx alpha, const double* scale, const double2* a,
                  long long lda, long long sa, const double2* b, long long ldb, long long sb,
                  cplx beta, double2* c, long long ldc, long long sc, cplx diag, int batch,
-                 const int* steps = nullptr, int step = 0, int reuse = 0) const {
+                 const int* steps = nullptr, int step = 0, int reuse = 0,
+                 const double2* cin = nullptr) const {
     if (precision == EUV_PREC_MIXED)
       return gemm_mixed(m, n, k, alpha, scale, a, lda, sa, b, ldb, sb, beta, c, ldc, sc, diag,
-                        batch, steps, step, mwork, mbytes, status, stream, reuse);
+                        batch, steps, step, mwork, mbytes, status, stream, reuse, cin);
+    if (cin != nullptr && cin != c) {
+      // FP64 GEMM: the beta term reads C, so C = Cin first (same shape)
+      const size_t span = (size_t)(batch - 1) * sc + (size_t)(n - 1) * ldc + m;
+      EUV_CUDA_TRY(cudaMemcpyAsync(c, cin, span * sizeof(double2), cudaMemcpyDeviceToDevice, stream));
+    }
     return zgemm(m, n, k, alpha, scale, a, lda, sa, b, ldb, sb, beta, c, ldc, sc, diag, batch,
                  steps, step, stream);
   }
@@ -872,8 +878,9 @@ extern "C" int euv_amp(const euv_amp_desc* d, const euv_c64* d_spectra, euv_c64*
       double2* t = P;
       P = Pn;
       Pn = t;
-      EUV_CUDA_TRY(cudaMemcpyAsync(Zt, Zc, (size_t)U * nn * sizeof(double2), cudaMemcpyDeviceToDevice, stream));
-      r2 = gemm(N, N, N, one, nullptr, P, N, nn, Zc, N, nn, one, Zt, N, nn, zero, U);
+      // Zt = P Zc + Zc (the beta term read from Zc)
+      r2 = gemm(N, N, N, one, nullptr, P, N, nn, Zc, N, nn, one, Zt, N, nn, zero, U, nullptr, 0, 0,
+                Zc);
       if (r2) return r2;
       t = Zc;
       Zc = Zt;
@@ -917,10 +924,10 @@ extern "C" int euv_amp(const euv_amp_desc* d, const euv_c64* d_spectra, euv_c64*
       build_dg_kernel<<<ge, bs, 0, stream>>>(qp, spec, d->d_spec, d->d_lindex, d->d_mindex,
                                              d->d_kx0, d->d_ky0, d->d_polar, nullptr, w.Gp, 0, 2);
       EUV_LAUNCH_CHECK();
-      EUV_CUDA_TRY(cudaMemcpyAsync(w.Z, X, (size_t)U * nn * sizeof(double2), cudaMemcpyDeviceToDevice, stream));
-      if ((rc = gemm(N, N, N, mk(-1.0, 0.0), nullptr, w.Gp, N, nn, X, N, nn, one, w.Z, N, nn, zero, U))) return rc;
-      EUV_CUDA_TRY(cudaMemcpyAsync(w.W, w.Z, (size_t)U * nn * sizeof(double2), cudaMemcpyDeviceToDevice, stream));
-      if ((rc = gemm(N, N, N, one, nullptr, w.G, N, nn, w.Z, N, nn, one, w.W, N, nn, zero, U))) return rc;
+      if ((rc = gemm(N, N, N, mk(-1.0, 0.0), nullptr, w.Gp, N, nn, X, N, nn, one, w.Z, N, nn, zero,
+                     U, nullptr, 0, 0, X))) return rc;  // Z = X - Gp X
+      if ((rc = gemm(N, N, N, one, nullptr, w.G, N, nn, w.Z, N, nn, one, w.W, N, nn, zero, U,
+                     nullptr, 0, 0, w.Z))) return rc;  // W = Z + G Z
       EUV_CUDA_TRY(cudaMemcpyAsync(w.Z, w.W, (size_t)U * nn * sizeof(double2), cudaMemcpyDeviceToDevice, stream));
       if ((rc = euler_tail(w.Z, true))) return rc;
       Zp = w.Z;
@@ -967,7 +974,14 @@ extern "C" int euv_amp(const euv_amp_desc* d, const euv_c64* d_spectra, euv_c64*
                      kReuseB))) return rc;  // Y as B again
       if ((rc = gemm(N, N, N, mi, nullptr, w.D, N, nn, Wb, N, nn, one, Yn, N, nn, zero, U))) return rc;
     }
-    // move the new X, Y into the dedicated buffers
+    if (n == 0) {
+      // top slice: the interface below reads Xn, Yn where they are (nothing
+      // after the loop writes the matrix-function buffers)
+      X = Xn;
+      Y = Yn;
+      break;
+    }
+    // move the new X, Y into the dedicated buffers for the next slice's matfun
     EUV_CUDA_TRY(cudaMemcpyAsync(w.X, Xn, (size_t)U * nn * sizeof(double2),
                                  cudaMemcpyDeviceToDevice, stream));
     EUV_CUDA_TRY(cudaMemcpyAsync(w.Y, Yn, (size_t)U * nn * sizeof(double2),

@@ -166,6 +166,26 @@ def test_mixed_precision_amplitudes(cuda, name):
     assert worst < MIXED_AMP_TOL
 
 
+@pytest.mark.parametrize("refresh", [False, True])
+def test_mixed_precision_sidewall_slices(cuda, refresh):
+    """Mixed form through several absorber slices, with the bottom slice's
+    sigma for all of them and with each slice's own."""
+    import torch
+    from euvlitho_b200.engine import Plan
+    cfg = preset("mixed").with_(refresh_sigma=refresh)
+    oc = to_oracle(cfg)
+    plan = Plan(cfg, device=cuda, pols=("X",), precision="mixed")
+    sl = _masks(cfg, [7], per_slice=True)[0]
+    ax, srcs = plan.amp(torch.from_numpy(np.stack([packed(m) for m in sl])[None]))
+    ax = ax.cpu().numpy()
+    L, M = cfg.order_limits()
+    ref = O.amp_s("X", [flat_bits(m) for m in sl], oc, plan.orders.lidx, plan.orders.midx, L, M,
+                  oc.kx0, oc.ky0)
+    worst = max(rel_err(ax[0, s], ref[key]) for s, key in enumerate(srcs))
+    print("mixed sidewall slices (refresh %s): max rel err %.2e" % (refresh, worst))
+    assert worst < MIXED_AMP_TOL
+
+
 # M3D parameters of the mixed form: ax, ay are least-squares slopes over the
 # sources that see a pupil order, and a slope can vanish (ax is ~1e-15 on this
 # clip: no x tilt of the chief ray), so every parameter's error is measured
