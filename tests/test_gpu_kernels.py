@@ -177,7 +177,8 @@ def test_mask_spectrum_batch(cuda):
         assert np.max(np.abs(got - ref)) < 1e-14, i
 
 
-@pytest.mark.parametrize("m,n,k,batch", [(128, 256, 16, 1), (121, 121, 121, 2), (300, 200, 77, 2), (961, 961, 961, 2)])
+@pytest.mark.parametrize("m,n,k,batch", [(128, 256, 16, 1), (121, 121, 121, 2), (300, 200, 77, 2), (961, 961, 961, 2),
+                                         (130, 144, 50, 1), (70, 16, 33, 1), (65, 130, 40, 3)])
 def test_zgemm_tf32x3(cuda, m, n, k, batch):
     """tcgen05 TF32x3 complex GEMM against NumPy FP64.  The bound is set by the
     FP32 accumulation in tensor memory (grows with K: ~1.5e-5 at K = 961)."""
