@@ -1,13 +1,15 @@
 // Mixed-precision complex GEMM on the 5th-generation tensor cores (tcgen05).
 //
 // C = alpha*scale[b] * A B + beta C + diag*I for complex FP64 A (MxK), B (KxN),
-// C (MxN), column-major and batched, computed as TF32x3: every FP64 real
+// C (MxN), column-major and batched (the beta term may read a separate Cin of
+// C's shape), computed as TF32x3: every FP64 real
 // operand is split into two TF32 values x = hi + lo (hi = x rounded to TF32,
 // lo = x - hi), and each real product is hi*hi + hi*lo + lo*hi with FP32
 // accumulation in tensor memory.  The complex product uses four real products:
 //   Re = ArBr - AiBi,  Im = ArBi + AiBr   (the minus sign through the MMA's
-//   negate-A bit), so one K=8 step issues 12 tcgen05.mma into a Re and an Im
-//   accumulator.  The FP32 accumulation error grows with the K it spans, so
+//   negate-A bit): twelve real TF32 products per K=8 step, issued as nine
+//   tcgen05.mma (the three Ar products as N = 256 against [Br | Bi], writing
+//   the adjacent Re and Im accumulators at once).  The FP32 accumulation error grows with the K it spans, so
 //   the two halves of K have their own Re/Im accumulators (four in all),
 //   summed in FP64 by the epilogue.
 // Error per product ~1e-6 relative: the bulk products of the slab matrix
