@@ -1001,8 +1001,11 @@ extern "C" int euv_amp(const euv_amp_desc* d, const euv_c64* d_spectra, euv_c64*
     src_rhs_kernel<<<gs, bs, 0, stream>>>(N, ns, d->d_src_order, d->d_src_2kz, w.E);
     EUV_LAUNCH_CHECK();
     if ((rc = lu_solve(N, ns, w.G, N, nn, w.ipiv, w.E, N, (long long)N * ns, U, stream))) return rc;
-    if ((rc = zgemm(N, ns, N, one, nullptr, Y, N, nn, w.E, N, (long long)N * ns, zero, w.YZ, N,
-                    (long long)N * ns, zero, U, nullptr, 0, stream)))
+    // Y Z for the source columns: a product, so the mixed form takes it on the
+    // tensor cores (TF32x3, ~1e-6 relative) like the matrix functions; the
+    // solve above stays FP64
+    if ((rc = gemm(N, ns, N, one, nullptr, Y, N, nn, w.E, N, (long long)N * ns, zero, w.YZ, N,
+                   (long long)N * ns, zero, U)))
       return rc;
     ax_out_kernel<<<gs, bs, 0, stream>>>(N, ns, d->d_src_order, w.klm, w.YZ,
                                          reinterpret_cast<double2*>(d_ax));
