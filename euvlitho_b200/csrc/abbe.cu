@@ -70,7 +70,23 @@ __device__ __forceinline__ void stage_x_lx(const double2* gp, cx<double> (&f)[AB
     f[e / 3][e % 3] = f[e / 3][e % 3] + cx<double>{v.x, v.y} * w;
   }
 }
-constexpr int AB_XPT = 4;  // x values per thread: xdiv <= 1024
+constexpr int AB_XPT = 4;  // x values (groups of four, radix-4) per thread: xdiv <= 1024
+constexpr int AB_GP = 4;   // radix-4 layout: zero rows of G before and after the pupil box
+static_assert(AB_YS == 4, "accumulators are [AB_XPT][4]");
+
+// the three components G[lx][b][0..2] of one row of the radix-4 layout (four
+// slots per (lx, b), 32 B aligned for FP32)
+__device__ __forceinline__ void load_g3(const float2* gp, cx<float> (&g)[3]) {
+  const float4 v0 = reinterpret_cast<const float4*>(gp)[0];
+  const float2 v1 = gp[2];
+  g[0] = {v0.x, v0.y};
+  g[1] = {v0.z, v0.w};
+  g[2] = {v1.x, v1.y};
+}
+__device__ __forceinline__ void load_g3(const double2* gp, cx<double> (&g)[3]) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c) g[c] = {gp[c].x, gp[c].y};
+}
 
 struct AbbeParams {
   int xdiv, ydiv, lpx, lpy, bx, by, ncut, n_src, n_order, nsplit;
@@ -84,15 +100,24 @@ struct AbbeParams {
   const double* inv_weight;
 };
 
-template <typename R>
+// R4: the x stage as four-way split sums (xdiv divisible by 4).  With
+// t = lx - lpx, f(g + q X/4) = sum_s i^(q s) P_s(g), P_s(g) = sum over t = s
+// (mod 4) of G(lx) e^(2 pi i t g / X): one pass over the pupil box gives four
+// image columns, combined by a radix-4 butterfly.  G then has AB_GP zero rows
+// on both sides and four slots per (lx, row), so the pass starts at an lx with
+// t = 0 (mod 4) and needs no bounds test.
+template <typename R, bool R4>
 __global__ void __launch_bounds__(AB_THREADS) abbe_kernel(AbbeParams p, const double2* ax,
                                                           double* image) {
   using V2 = typename vec2<R>::type;
   using C = cx<R>;
+  constexpr int GC = R4 ? 4 : 3;       // slots per (lx, row)
+  constexpr int GP = R4 ? AB_GP : 0;   // zero rows before the pupil box
   extern __shared__ __align__(16) unsigned char sm_raw[];
   V2* E = reinterpret_cast<V2*>(sm_raw);              // [ncut][3]
-  V2* G = E + (((size_t)p.ncut * 3 + 1) & ~(size_t)1);  // [bx][YS][3], 16 B aligned
-  V2* twy = G + (size_t)AB_YS * p.bx * 3;             // [YS][by]
+  V2* G = E + (((size_t)p.ncut * 3 + 1) & ~(size_t)1);  // [GP + bx + GP][YS][GC], 16 B aligned
+  const int g_rows = p.bx + 2 * GP;
+  V2* twy = G + (size_t)g_rows * AB_YS * GC;          // [YS][by]
   int* s_py = reinterpret_cast<int*>(twy + (size_t)AB_YS * p.by);  // [ncut] pupil m + lpy
   const int u = blockIdx.z;
   const int y0 = blockIdx.x * AB_YS;
@@ -110,12 +135,14 @@ __global__ void __launch_bounds__(AB_THREADS) abbe_kernel(AbbeParams p, const do
     twy[idx] = V2{(R)c, (R)s};
   }
   for (int i = tid; i < p.ncut; i += AB_THREADS) s_py[i] = p.py[i] + p.lpy;
+  if (R4)  // the pad rows and slots stay zero; stage y writes the rest
+    for (int i = tid; i < g_rows * AB_YS * GC; i += AB_THREADS) G[i] = V2{(R)0, (R)0};
 
-  double acc[AB_XPT][AB_YS];
+  double acc[AB_XPT][4];
 #pragma unroll
   for (int a = 0; a < AB_XPT; ++a)
 #pragma unroll
-    for (int b = 0; b < AB_YS; ++b) acc[a][b] = 0.0;
+    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
 
   for (int s = blockIdx.y; s < nsrc_u; s += p.nsplit) {
     __syncthreads();
@@ -137,7 +164,7 @@ __global__ void __launch_bounds__(AB_THREADS) abbe_kernel(AbbeParams p, const do
       E[i * 3 + 2] = V2{(R)e2.x, (R)e2.y};
     }
     __syncthreads();
-    // stage y; G[lx][yy][c]: the 3 AB_YS values stage x reads per lx are contiguous
+    // stage y; G[GP + lx][yy][c]: the values stage x reads per lx are contiguous
     for (int o = tid; o < AB_YS * p.bx * 3; o += AB_THREADS) {
       const int c = o % 3, lx = (o / 3) % p.bx, yy = o / (3 * p.bx);
       C g{(R)0, (R)0};
@@ -148,45 +175,107 @@ __global__ void __launch_bounds__(AB_THREADS) abbe_kernel(AbbeParams p, const do
         const V2 t = ty[s_py[i]];
         g = g + C{e.x, e.y} * C{t.x, t.y};
       }
-      G[(lx * AB_YS + yy) * 3 + c] = V2{g.x, g.y};
+      G[((GP + lx) * AB_YS + yy) * GC + c] = V2{g.x, g.y};
     }
     __syncthreads();
-    // stage x + |f|^2
+    if (R4) {
+      // stage x, radix 4: thread = (column group g, stripe row b)
+      const int b = tid & (AB_YS - 1), g0 = tid / AB_YS;
+      const int x4 = p.xdiv / 4;
+      const int lx0 = (p.lpx & 3) - 4;  // lx0 - lpx = 0 (mod 4); rows lx0 .. -1 are pad
+      const int nj = (p.bx - lx0 + 3) / 4;
 #pragma unroll
-    for (int a = 0; a < AB_XPT; ++a) {
-      const int x = tid + a * AB_THREADS;
-      if (x < p.xdiv) {
-        long long q0 = ((long long)(-p.lpx) * x) % p.xdiv;
-        if (q0 < 0) q0 += p.xdiv;
-        double s0, c0, s1, c1;
-        sincospi(2.0 * (double)q0 / (double)p.xdiv, &s0, &c0);
-        sincospi(2.0 * (double)x / (double)p.xdiv, &s1, &c1);
-        C w{(R)c0, (R)s0};
-        const C r{(R)c1, (R)s1};
-        C f[AB_YS][3];
+      for (int a = 0; a < AB_XPT; ++a) {
+        const int g = g0 + a * (AB_THREADS / AB_YS);
+        if (g < x4) {
+          long long q0 = ((long long)(lx0 - p.lpx) * g) % p.xdiv;
+          if (q0 < 0) q0 += p.xdiv;
+          double s0, c0, s1, c1;
+          sincospi(2.0 * (double)q0 / (double)p.xdiv, &s0, &c0);
+          sincospi(2.0 * (double)g / (double)p.xdiv, &s1, &c1);
+          C w{(R)c0, (R)s0};
+          const C r{(R)c1, (R)s1};
+          C P[4][3];
 #pragma unroll
-        for (int b = 0; b < AB_YS; ++b) f[b][0] = f[b][1] = f[b][2] = C{(R)0, (R)0};
-        const V2* gp = G;
-        for (int lx = 0; lx < p.bx; ++lx, gp += AB_YS * 3) {
-          stage_x_lx(gp, f, w);
-          w = w * r;
+          for (int k = 0; k < 4; ++k) P[k][0] = P[k][1] = P[k][2] = C{(R)0, (R)0};
+          const V2* gp = G + ((size_t)(GP + lx0) * AB_YS + b) * GC;
+          for (int j = 0; j < nj; ++j) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k, gp += AB_YS * GC) {
+              C gv[3];
+              load_g3(gp, gv);
+#pragma unroll
+              for (int c = 0; c < 3; ++c) P[k][c] = P[k][c] + gv[c] * w;
+              w = w * r;
+            }
+          }
+          double e[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const C A{P[0][c].x + P[2][c].x, P[0][c].y + P[2][c].y};
+            const C B{P[0][c].x - P[2][c].x, P[0][c].y - P[2][c].y};
+            const C S{P[1][c].x + P[3][c].x, P[1][c].y + P[3][c].y};
+            const C D{P[1][c].x - P[3][c].x, P[1][c].y - P[3][c].y};
+            const C f[4] = {{A.x + S.x, A.y + S.y}, {B.x - D.y, B.y + D.x},
+                            {A.x - S.x, A.y - S.y}, {B.x + D.y, B.y - D.x}};
+#pragma unroll
+            for (int q = 0; q < 4; ++q) e[q] += (double)(f[q].x * f[q].x + f[q].y * f[q].y);
+          }
+#pragma unroll
+          for (int q = 0; q < 4; ++q) acc[a][q] += e[q];
         }
+      }
+    } else {
+      // stage x + |f|^2, one image column per thread
 #pragma unroll
-        for (int b = 0; b < AB_YS; ++b)
-          acc[a][b] += (double)(f[b][0].x * f[b][0].x + f[b][0].y * f[b][0].y + f[b][1].x * f[b][1].x +
-                                f[b][1].y * f[b][1].y + f[b][2].x * f[b][2].x + f[b][2].y * f[b][2].y);
+      for (int a = 0; a < AB_XPT; ++a) {
+        const int x = tid + a * AB_THREADS;
+        if (x < p.xdiv) {
+          long long q0 = ((long long)(-p.lpx) * x) % p.xdiv;
+          if (q0 < 0) q0 += p.xdiv;
+          double s0, c0, s1, c1;
+          sincospi(2.0 * (double)q0 / (double)p.xdiv, &s0, &c0);
+          sincospi(2.0 * (double)x / (double)p.xdiv, &s1, &c1);
+          C w{(R)c0, (R)s0};
+          const C r{(R)c1, (R)s1};
+          C f[AB_YS][3];
+#pragma unroll
+          for (int b = 0; b < AB_YS; ++b) f[b][0] = f[b][1] = f[b][2] = C{(R)0, (R)0};
+          const V2* gp = G;
+          for (int lx = 0; lx < p.bx; ++lx, gp += AB_YS * 3) {
+            stage_x_lx(gp, f, w);
+            w = w * r;
+          }
+#pragma unroll
+          for (int b = 0; b < AB_YS; ++b)
+            acc[a][b] += (double)(f[b][0].x * f[b][0].x + f[b][0].y * f[b][0].y +
+                                  f[b][1].x * f[b][1].x + f[b][1].y * f[b][1].y +
+                                  f[b][2].x * f[b][2].x + f[b][2].y * f[b][2].y);
+        }
       }
     }
   }
   const double wgt = p.inv_weight[img];
   double* im = image + (size_t)img * p.xdiv * p.ydiv;
+  if (R4) {
+    const int b = tid & (AB_YS - 1), g0 = tid / AB_YS, x4 = p.xdiv / 4;
 #pragma unroll
-  for (int a = 0; a < AB_XPT; ++a) {
-    const int x = tid + a * AB_THREADS;
-    if (x < p.xdiv)
+    for (int a = 0; a < AB_XPT; ++a) {
+      const int g = g0 + a * (AB_THREADS / AB_YS);
+      if (g < x4 && b < ny)
 #pragma unroll
-      for (int b = 0; b < AB_YS; ++b)
-        if (b < ny) atomicAdd(&im[(size_t)x * p.ydiv + y0 + b], acc[a][b] * wgt);
+        for (int q = 0; q < 4; ++q)
+          atomicAdd(&im[(size_t)(g + q * x4) * p.ydiv + y0 + b], acc[a][q] * wgt);
+    }
+  } else {
+#pragma unroll
+    for (int a = 0; a < AB_XPT; ++a) {
+      const int x = tid + a * AB_THREADS;
+      if (x < p.xdiv)
+#pragma unroll
+        for (int b = 0; b < AB_YS; ++b)
+          if (b < ny) atomicAdd(&im[(size_t)x * p.ydiv + y0 + b], acc[a][b] * wgt);
+    }
   }
 }
 
@@ -230,24 +319,33 @@ extern "C" int euv_abbe(const euv_abbe_desc* d, const euv_c64* d_ax, double* d_i
   if (nsplit > d->n_src) nsplit = d->n_src;
   p.nsplit = nsplit;
   const bool fp32 = d->precision == EUV_PREC_MIXED;
-  size_t smem = ((((size_t)d->ncut * 3 + 1) & ~(size_t)1) + (size_t)AB_YS * p.bx * 3 +
-                 (size_t)AB_YS * p.by) * (fp32 ? sizeof(float2) : sizeof(double2)) +
-                 (size_t)d->ncut * sizeof(int);
+  const bool r4 = d->xdiv % 4 == 0;
+  const size_t g_elems = r4 ? (size_t)(p.bx + 2 * AB_GP) * AB_YS * 4 : (size_t)AB_YS * p.bx * 3;
+  size_t smem = ((((size_t)d->ncut * 3 + 1) & ~(size_t)1) + g_elems + (size_t)AB_YS * p.by) *
+                    (fp32 ? sizeof(float2) : sizeof(double2)) +
+                (size_t)d->ncut * sizeof(int);
   if (smem > 227 * 1024) {
     euv_set_error("euv_abbe: pupil too large for one CTA (%zu bytes of shared memory)", smem);
     return EUV_ERR_BAD_ARG;
   }
   dim3 grid(ystripes, nsplit, d->n_units);
-  if (fp32) {
+  const double2* axp = reinterpret_cast<const double2*>(d_ax);
+  if (fp32 && r4) {
     static int smem_done[64];
-    EUV_CUDA_TRY(ensure_smem(abbe_kernel<float>, (int)smem, smem_done));
-    abbe_kernel<float><<<grid, AB_THREADS, smem, stream>>>(p, reinterpret_cast<const double2*>(d_ax),
-                                                           d_image);
+    EUV_CUDA_TRY(ensure_smem(abbe_kernel<float, true>, (int)smem, smem_done));
+    abbe_kernel<float, true><<<grid, AB_THREADS, smem, stream>>>(p, axp, d_image);
+  } else if (fp32) {
+    static int smem_done[64];
+    EUV_CUDA_TRY(ensure_smem(abbe_kernel<float, false>, (int)smem, smem_done));
+    abbe_kernel<float, false><<<grid, AB_THREADS, smem, stream>>>(p, axp, d_image);
+  } else if (r4) {
+    static int smem_done[64];
+    EUV_CUDA_TRY(ensure_smem(abbe_kernel<double, true>, (int)smem, smem_done));
+    abbe_kernel<double, true><<<grid, AB_THREADS, smem, stream>>>(p, axp, d_image);
   } else {
     static int smem_done[64];
-    EUV_CUDA_TRY(ensure_smem(abbe_kernel<double>, (int)smem, smem_done));
-    abbe_kernel<double><<<grid, AB_THREADS, smem, stream>>>(p, reinterpret_cast<const double2*>(d_ax),
-                                                            d_image);
+    EUV_CUDA_TRY(ensure_smem(abbe_kernel<double, false>, (int)smem, smem_done));
+    abbe_kernel<double, false><<<grid, AB_THREADS, smem, stream>>>(p, axp, d_image);
   }
   EUV_LAUNCH_CHECK();
   return EUV_OK;

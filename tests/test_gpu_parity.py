@@ -98,6 +98,21 @@ def test_intensity_matches_oracle(cuda, pols):
             assert rel_err(img[c, p], ref[pol]) < TOL
 
 
+@pytest.mark.parametrize("ndivx", [232, 264, 300, 304, 352, 400])
+def test_intensity_image_widths(cuda, ndivx):
+    """Image widths XDIV = NDIVX/4 = 58, 66, 75 (one column per thread in the x
+    stage) and 76, 88, 100 (the four-column split, XDIV divisible by 4, with
+    pupil half-widths 6, 7, 8: every residue mod 4 with the default's 5)."""
+    import torch
+    cfg = preset("small").with_(ndivx=ndivx)
+    oc = to_oracle(cfg)
+    plan = _plan(cfg, cuda)
+    m = random_mask(cfg.ndivx, cfg.ndivy, seed=ndivx)
+    img = plan.intensity(torch.from_numpy(packed(m)[None])).cpu().numpy()
+    ref = O.intensity(oc, flat_bits(m), polars=("X",))
+    assert rel_err(img[0, 0], ref["X"]) < TOL
+
+
 def test_intensity_same_alone_and_batched(cuda):
     """A clip's image does not depend on the other clips in the launch."""
     import torch
