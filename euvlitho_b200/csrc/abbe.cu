@@ -100,12 +100,15 @@ struct AbbeParams {
   const double* inv_weight;
 };
 
-// R4: the x stage as four-way split sums (xdiv divisible by 4).  With
-// t = lx - lpx, f(g + q X/4) = sum_s i^(q s) P_s(g), P_s(g) = sum over t = s
-// (mod 4) of G(lx) e^(2 pi i t g / X): one pass over the pupil box gives four
-// image columns, combined by a radix-4 butterfly.  G then has AB_GP zero rows
-// on both sides and four slots per (lx, row), so the pass starts at an lx with
-// t = 0 (mod 4) and needs no bounds test.
+// R4 (xdiv and ydiv divisible by 4): both DFT stages as four-way splits.
+//   x stage: with t = lx - lpx, f(g + q X/4) = sum_s i^(q s) P_s(g), P_s(g) =
+//     sum over t = s (mod 4) of G(lx) e^(2 pi i t g / X): one pass over the
+//     pupil box gives four image columns, combined by a radix-4 butterfly.  G
+//     has AB_GP zero rows on both sides and four slots per (lx, row), so the
+//     pass starts at an lx with t = 0 (mod 4) and needs no bounds test.
+//   y stage: the CTA's four rows are y0 + q Y/4 (not four adjacent rows), so
+//     with u = E(l, m) e^(2 pi i m y0 / Y) every pupil point adds i^(m q) u to
+//     row q: one product per point for the four rows.
 template <typename R, bool R4>
 __global__ void __launch_bounds__(AB_THREADS) abbe_kernel(AbbeParams p, const double2* ax,
                                                           double* image) {
@@ -120,13 +123,15 @@ __global__ void __launch_bounds__(AB_THREADS) abbe_kernel(AbbeParams p, const do
   V2* twy = G + (size_t)g_rows * AB_YS * GC;          // [YS][by]
   int* s_py = reinterpret_cast<int*>(twy + (size_t)AB_YS * p.by);  // [ncut] pupil m + lpy
   const int u = blockIdx.z;
-  const int y0 = blockIdx.x * AB_YS;
+  const int y0 = R4 ? blockIdx.x : blockIdx.x * AB_YS;
+  const int ystep = R4 ? p.ydiv / 4 : 1;  // distance between the CTA's image rows
   const int tid = threadIdx.x;
   const int nsrc_u = p.nsrc_of_unit[u];
   const int img = p.img_of_unit[u];
-  const int ny = (p.ydiv - y0) < AB_YS ? (p.ydiv - y0) : AB_YS;
+  const int ny = R4 ? AB_YS : ((p.ydiv - y0) < AB_YS ? (p.ydiv - y0) : AB_YS);
 
-  for (int idx = tid; idx < AB_YS * p.by; idx += AB_THREADS) {
+  // twiddles of stage y: rows y0 + yy (R4: the one row y0)
+  for (int idx = tid; idx < (R4 ? 1 : AB_YS) * p.by; idx += AB_THREADS) {
     int yy = idx / p.by, mm = idx % p.by;
     long long q = ((long long)(mm - p.lpy) * (y0 + yy)) % p.ydiv;
     if (q < 0) q += p.ydiv;
@@ -165,6 +170,43 @@ __global__ void __launch_bounds__(AB_THREADS) abbe_kernel(AbbeParams p, const do
     }
     __syncthreads();
     // stage y; G[GP + lx][yy][c]: the values stage x reads per lx are contiguous
+    if (R4) {
+      const int kofs = 4 - (p.lpy & 3);  // (mm + kofs) & 3 = (mm - lpy) mod 4 = m mod 4
+      // two lanes per (lx, c): alternate points, summed by a shuffle
+      const int nitem2 = 2 * p.bx * 3;
+      for (int base = 0; base < nitem2; base += AB_THREADS) {  // uniform trip count
+        const int o = base + tid;
+        const bool live = o < nitem2;
+        const int item = o >> 1, c = item % 3, lx = item / 3;
+        C g[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) g[q] = C{(R)0, (R)0};
+        const int i0 = live ? p.row_start[lx] + (o & 1) : 0, i1 = live ? p.row_start[lx + 1] : 0;
+        for (int i = i0; i < i1; i += 2) {
+          const V2 e = E[i * 3 + c];
+          const int mm = s_py[i];
+          const V2 t = twy[mm];
+          const C w = C{e.x, e.y} * C{t.x, t.y};
+          const int k = (mm + kofs) & 3;
+          // i^k w = sg (i^(k&1) w); (-1)^k w; (-i)^k w = (-1)^k sg (i^(k&1) w)
+          const C v = (k & 1) ? C{-w.y, w.x} : w;
+          const R sg = (k & 2) ? (R)-1 : (R)1;
+          const R sodd = (k & 1) ? (R)-1 : (R)1;
+          g[0] = C{g[0].x + w.x, g[0].y + w.y};
+          g[1] = C{g[1].x + sg * v.x, g[1].y + sg * v.y};
+          g[2] = C{g[2].x + sodd * w.x, g[2].y + sodd * w.y};
+          g[3] = C{g[3].x + sodd * sg * v.x, g[3].y + sodd * sg * v.y};
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          g[q].x += __shfl_xor_sync(0xffffffffu, g[q].x, 1);
+          g[q].y += __shfl_xor_sync(0xffffffffu, g[q].y, 1);
+        }
+        if (live && (o & 1) == 0)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) G[((GP + lx) * AB_YS + q) * GC + c] = V2{g[q].x, g[q].y};
+      }
+    } else
     for (int o = tid; o < AB_YS * p.bx * 3; o += AB_THREADS) {
       const int c = o % 3, lx = (o / 3) % p.bx, yy = o / (3 * p.bx);
       C g{(R)0, (R)0};
@@ -265,7 +307,7 @@ __global__ void __launch_bounds__(AB_THREADS) abbe_kernel(AbbeParams p, const do
       if (g < x4 && b < ny)
 #pragma unroll
         for (int q = 0; q < 4; ++q)
-          atomicAdd(&im[(size_t)(g + q * x4) * p.ydiv + y0 + b], acc[a][q] * wgt);
+          atomicAdd(&im[(size_t)(g + q * x4) * p.ydiv + y0 + b * ystep], acc[a][q] * wgt);
     }
   } else {
 #pragma unroll
@@ -319,7 +361,7 @@ extern "C" int euv_abbe(const euv_abbe_desc* d, const euv_c64* d_ax, double* d_i
   if (nsplit > d->n_src) nsplit = d->n_src;
   p.nsplit = nsplit;
   const bool fp32 = d->precision == EUV_PREC_MIXED;
-  const bool r4 = d->xdiv % 4 == 0;
+  const bool r4 = d->xdiv % 4 == 0 && d->ydiv % 4 == 0;
   const size_t g_elems = r4 ? (size_t)(p.bx + 2 * AB_GP) * AB_YS * 4 : (size_t)AB_YS * p.bx * 3;
   size_t smem = ((((size_t)d->ncut * 3 + 1) & ~(size_t)1) + g_elems + (size_t)AB_YS * p.by) *
                     (fp32 ? sizeof(float2) : sizeof(double2)) +

@@ -98,16 +98,20 @@ def test_intensity_matches_oracle(cuda, pols):
             assert rel_err(img[c, p], ref[pol]) < TOL
 
 
-@pytest.mark.parametrize("ndivx", [232, 264, 300, 304, 352, 400])
-def test_intensity_image_widths(cuda, ndivx):
-    """Image widths XDIV = NDIVX/4 = 58, 66, 75 (one column per thread in the x
-    stage) and 76, 88, 100 (the four-column split, XDIV divisible by 4, with
-    pupil half-widths 6, 7, 8: every residue mod 4 with the default's 5)."""
+@pytest.mark.parametrize("ndivx,ndivy", [(232, 256), (264, 256), (300, 256), (304, 256), (352, 256),
+                                         (400, 256), (256, 264), (256, 288), (256, 320), (256, 416),
+                                         (256, 512)])
+def test_intensity_image_sizes(cuda, ndivx, ndivy):
+    """Image sizes XDIV x YDIV = NDIVX/4 x NDIVY/8.  Widths 58, 66, 75 take the
+    one-column-per-thread x stage; 76, 88, 100 the four-way split (XDIV and
+    YDIV divisible by 4) with pupil half-widths 6, 7, 8 (every residue mod 4
+    with the default's 5); heights 33 (no split), 36, 40, 52, 64 (split y
+    stage, a CTA's rows Y/4 apart, pupil half-heights 2, 3, 4, 5)."""
     import torch
-    cfg = preset("small").with_(ndivx=ndivx)
+    cfg = preset("small").with_(ndivx=ndivx, ndivy=ndivy)
     oc = to_oracle(cfg)
     plan = _plan(cfg, cuda)
-    m = random_mask(cfg.ndivx, cfg.ndivy, seed=ndivx)
+    m = random_mask(cfg.ndivx, cfg.ndivy, seed=ndivx + ndivy)
     img = plan.intensity(torch.from_numpy(packed(m)[None])).cpu().numpy()
     ref = O.intensity(oc, flat_bits(m), polars=("X",))
     assert rel_err(img[0, 0], ref["X"]) < TOL
