@@ -356,10 +356,6 @@ extern "C" int euv_abbe(const euv_abbe_desc* d, const euv_c64* d_ax, double* d_i
   p.nsrc_of_unit = d->d_nsrc_of_unit;
   p.inv_weight = d->d_inv_weight;
   const int ystripes = (d->ydiv + AB_YS - 1) / AB_YS;
-  int nsplit = (2 * 148 + ystripes * d->n_units - 1) / (ystripes * d->n_units);
-  if (nsplit < 1) nsplit = 1;
-  if (nsplit > d->n_src) nsplit = d->n_src;
-  p.nsplit = nsplit;
   const bool fp32 = d->precision == EUV_PREC_MIXED;
   const bool r4 = d->xdiv % 4 == 0 && d->ydiv % 4 == 0;
   const size_t g_elems = r4 ? (size_t)(p.bx + 2 * AB_GP) * AB_YS * 4 : (size_t)AB_YS * p.bx * 3;
@@ -370,25 +366,35 @@ extern "C" int euv_abbe(const euv_abbe_desc* d, const euv_c64* d_ax, double* d_i
     euv_set_error("euv_abbe: pupil too large for one CTA (%zu bytes of shared memory)", smem);
     return EUV_ERR_BAD_ARG;
   }
-  dim3 grid(ystripes, nsplit, d->n_units);
-  const double2* axp = reinterpret_cast<const double2*>(d_ax);
-  if (fp32 && r4) {
-    static int smem_done[64];
-    EUV_CUDA_TRY(ensure_smem(abbe_kernel<float, true>, (int)smem, smem_done));
-    abbe_kernel<float, true><<<grid, AB_THREADS, smem, stream>>>(p, axp, d_image);
-  } else if (fp32) {
-    static int smem_done[64];
-    EUV_CUDA_TRY(ensure_smem(abbe_kernel<float, false>, (int)smem, smem_done));
-    abbe_kernel<float, false><<<grid, AB_THREADS, smem, stream>>>(p, axp, d_image);
-  } else if (r4) {
-    static int smem_done[64];
-    EUV_CUDA_TRY(ensure_smem(abbe_kernel<double, true>, (int)smem, smem_done));
-    abbe_kernel<double, true><<<grid, AB_THREADS, smem, stream>>>(p, axp, d_image);
-  } else {
-    static int smem_done[64];
-    EUV_CUDA_TRY(ensure_smem(abbe_kernel<double, false>, (int)smem, smem_done));
-    abbe_kernel<double, false><<<grid, AB_THREADS, smem, stream>>>(p, axp, d_image);
+  using Kern = void (*)(AbbeParams, const double2*, double*);
+  static const Kern kerns[4] = {abbe_kernel<double, false>, abbe_kernel<double, true>,
+                                abbe_kernel<float, false>, abbe_kernel<float, true>};
+  static int smem_done[4][64];
+  const int kv = (fp32 ? 2 : 0) + (r4 ? 1 : 0);
+  EUV_CUDA_TRY(ensure_smem(kerns[kv], (int)smem, smem_done[kv]));
+  // source split: the CTAs of a unit's row groups take every nsplit-th source.
+  // Chosen to minimise (waves of resident CTAs) x (sources per CTA + 1), the
+  // 1 standing for a CTA's own setup and atomics, so that the last wave is not
+  // left mostly empty without multiplying the CTAs; ties keep the smaller
+  // split.
+  int dev = 0, sms = 148, per_sm = 1;
+  EUV_CUDA_TRY(cudaGetDevice(&dev));
+  EUV_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  EUV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kerns[kv], AB_THREADS, smem));
+  const long long slots = (long long)sms * (per_sm > 0 ? per_sm : 1);
+  const long long groups = (long long)ystripes * d->n_units;
+  int nsplit = 1;
+  long long best = -1;
+  for (int ns = 1; ns <= d->n_src && ns <= 64; ++ns) {
+    const long long cost = ((groups * ns + slots - 1) / slots) * ((d->n_src + ns - 1) / ns + 1);
+    if (best < 0 || cost < best) {
+      best = cost;
+      nsplit = ns;
+    }
   }
+  p.nsplit = nsplit;
+  dim3 grid(ystripes, nsplit, d->n_units);
+  kerns[kv]<<<grid, AB_THREADS, smem, stream>>>(p, reinterpret_cast<const double2*>(d_ax), d_image);
   EUV_LAUNCH_CHECK();
   return EUV_OK;
 }
