@@ -42,11 +42,11 @@ int gemm_mixed(int m, int n, int k, cplx alpha, const double* scale, const doubl
 size_t gemm_mixed_workspace_bytes(int m, int n, int k, int batch);
 
 // ||A||_1 bound for the degree-8 Taylor step of cos/sin(sqrt(A)): the dropped
-// term is ~theta^9/18!, 1.6e-16 at theta = 1 (FP64) and 4e-11 at theta = 4,
+// term is ~theta^9/18!, 1.6e-16 at theta = 1 (FP64) and 2e-8 at theta = 8,
 // which the mixed form uses (its TF32x3 products carry ~1e-6 relative error,
 // and each double-angle step saved also saves its error growth).
 constexpr double kThetaFp64 = 1.0;
-constexpr double kThetaMixed = 4.0;
+constexpr double kThetaMixed = 8.0;
 inline double theta_for(int precision) {
   return precision == EUV_PREC_MIXED ? kThetaMixed : kThetaFp64;
 }
