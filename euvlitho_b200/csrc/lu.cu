@@ -138,15 +138,15 @@ __global__ void __launch_bounds__(LU_PANEL_THREADS) lu_panel_kernel(int n, int j
 // memory, one column per lane of the warp that holds the row, and rank 0 sends
 // row jj the same way; after it, every thread reduces the LC candidates in
 // rank order (same pivot in every CTA), takes the pivot row from the winner's
-// slot, swaps, scales and applies the rank-1 update to its own row.  Slots
-// alternate by column parity: a slot is rewritten two barriers after it was
-// read.  A block's columns are stored when it ends (final apart from later row
-// swaps), pivots and the singular flag when the panel ends.  Columns of rows
-// swapped by later pivots, and the columns left of the block of rows swapped
-// inside it, are fixed by the laswp launch after the panel (sub = 1: column c
-// gets the swaps of pivots c+1..).  Every thread executes every barrier the
-// same number of times whatever the data (a zero pivot skips only the
-// arithmetic).
+// slot, swaps, scales and applies the rank-1 update to its own row.  The swap
+// at column jj exchanges only the columns from jj on (the part of the two rows
+// the remaining columns use), so every column c of the panel holds the swaps of
+// pivots ..c and lacks exactly those of pivots c+1..: the laswp launch after the
+// panel applies them (sub = 1).  Slots alternate by column parity: a slot is
+// rewritten two barriers after it was read.  A block's columns are stored when
+// it ends, pivots and the singular flag when the panel ends.  Every thread
+// executes every barrier the same number of times whatever the data (a zero
+// pivot skips only the arithmetic).
 constexpr int LC_THREADS = 256;
 constexpr int LC_WARPS = LC_THREADS / 32;
 constexpr int LC_BLK = 4;
