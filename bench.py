@@ -159,6 +159,29 @@ def _traffic(name: str):
         return None
 
 
+def _measured_peaks():
+    """The GPU pool's measured peaks (MEASURED_PEAKS.json beside this file, written
+    per pod; None if absent).  It holds HBM and bf16 rates, no TF32 rate."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            mp = json.load(f)
+        return mp if isinstance(mp, dict) else None
+    except (OSError, ValueError):
+        return None
+
+
+def _with_measured_peaks(out: dict, achieved: float) -> dict:
+    """Adds the measured-peaks file and the fraction of its dense bf16 rate (the
+    file's only tensor figure; a TF32 kernel's own bound is the in-run TF32 rate)."""
+    mp = _measured_peaks()
+    if mp is not None:
+        out["measured_peaks_file"] = mp
+        bf = mp.get("bf16_tflops")
+        if isinstance(bf, (int, float)) and bf > 0:
+            out["frac_of_measured_bf16"] = achieved / float(bf)
+    return out
+
+
 def dominant_kernel_roofline(plan, U, precision, dev, stream, L):
     """Roofline of the step's dominant kernel at the pipeline's shape (all U
     units of N orders), timed live with CUDA events on the launching stream.
@@ -212,7 +235,7 @@ def dominant_kernel_roofline(plan, U, precision, dev, stream, L):
     achieved = flop / (ms / 1e3) / 1e12
     out.update({"achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                 "ms_per_launch": ms, "algorithmic_flop_per_launch": flop})
-    return out
+    return _with_measured_peaks(out, achieved)
 
 
 def library_path_sample(plan, masks_dev, dev, units_per_clip: int, n_src_images: int):
