@@ -17,6 +17,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -29,9 +30,10 @@ sys.path.insert(0, ROOT)
 
 METRIC = "clips/s + p99 latency vs plain FP64 path on 1 B200 at <=1e-4 intensity error"
 CLIPS = 4
-WORKLOAD = ("batched: 4 clips/step of 1024x1024 nm on a 1024^2 grid, NA 0.55 4x/8x, orders 31x31 "
-            "(N=961 per polarisation), 200-point annular source sigma 0.5-0.9 (3 Bloch families), "
-            "X+Y polarisation, 60 nm absorber n=0.95+0.031i, Ru cap + 40 Mo/Si")
+_CLIP = ("1024x1024 nm on a 1024^2 grid, NA 0.55 4x/8x, orders 31x31 (N=961 per polarisation), "
+         "200-point annular source sigma 0.5-0.9 (3 Bloch families), X+Y polarisation, 60 nm "
+         "absorber n=0.95+0.031i, Ru cap + 40 Mo/Si")
+WORKLOAD = "batched: seeded clips of " + _CLIP
 
 
 def _args():
@@ -48,69 +50,73 @@ def _args():
 
 
 # ---------------------------------------------------------------- CPU (oracle)
-def cpu_sample(seconds_hint: float = 10.0):
-    """Time the oracle (FP64 NumPy/LAPACK port of the reference) on a bounded
-    sample of the workload and scale to clips/s: one (family, polarisation)
-    ampS at N=961 plus the Abbe fields + 3 inverse FFTs of 4 source points."""
+def _cpu_threads() -> int:
+    return len(os.sched_getaffinity(0))
+
+
+def cpu_clip(seed: int):
+    """One whole clip of the workload through the oracle (the reference's
+    algorithm restated in NumPy/LAPACK FP64, all host threads through the BLAS):
+    every (family, polarisation) ampS at N = 961 and the Abbe images of both
+    polarisations over all source points.  Returns (seconds, images[pol])."""
     import numpy as np
     from euvlitho_b200 import masks as MK
     from euvlitho_b200.config import preset
     from oracle import euv_oracle as O
     from tests.helpers import to_oracle
     cfg = preset("batched")
+    m = MK.synth_mask(cfg.ndivx, cfg.ndivy, seed).reshape(-1).astype(np.int32)
     oc = to_oracle(cfg)
-    m = MK.synth_mask(cfg.ndivx, cfg.ndivy, seed=1).reshape(-1).astype(np.int32)
-    L_, M_ = cfg.order_limits()
-    li, mi = O.order_set(cfg.order_kind, L_, M_)
-    ndivs, fams = O.source(oc)
-    fams = [(k, v) for k, v in fams.items() if v]
-    lin, mn, _, _ = O.pupil_set(oc)
-    (nsx, nsy), pts = fams[0]
-    sx0 = 2 * O.PI / oc.dx * nsx / ndivs + oc.kx0
-    sy0 = 2 * O.PI / oc.dy * nsy / ndivs + oc.ky0
     t0 = time.perf_counter()
-    Ax = O.amp_s("X", m, oc, li, mi, L_, M_, sx0, sy0, source_orders=pts)
-    t_unit = time.perf_counter() - t0
-    nsrc = 4
-    t1 = time.perf_counter()
-    Fs = O.abbe_family_fields(oc, "X", Ax, li, mi, nsx, nsy, ndivs, pts[:nsrc], lin, mn, 0)
-    for F in Fs:
-        f = np.fft.ifft2(F, axes=(1, 2)) * (oc.xdiv * oc.ydiv)
-        _ = np.sum(f.real ** 2 + f.imag ** 2, axis=0)
-    t_src = (time.perf_counter() - t1) / nsrc
-    units_per_clip = len(fams) * 2
-    src_per_clip = sum(len(v) for _, v in fams) * 2
-    t_clip = units_per_clip * t_unit + src_per_clip * t_src
-    cores = len(os.sched_getaffinity(0))
-    return {
-        "value": 1.0 / t_clip, "unit": "clips/s", "cores": cores, "kind": "port",
-        "sample": "oracle (NumPy/LAPACK FP64) on %d threads: one N=961 ampS (%.2f s) and the Abbe "
-                  "fields of %d source points (%.3f s each), scaled to one clip = %d ampS + %d "
-                  "source images" % (cores, t_unit, nsrc, t_src, units_per_clip, src_per_clip),
-    }
+    img = O.intensity(oc, m, polars=("X", "Y"))
+    return time.perf_counter() - t0, img
+
+
+def _clip_sample_text(cfg_units: int, cfg_src: int) -> str:
+    return ("oracle (NumPy/LAPACK FP64) on %d threads: one whole clip per sample = %d ampS of "
+            "N=961 + Abbe images of %d source points x 2 polarisations"
+            % (_cpu_threads(), cfg_units, cfg_src))
 
 
 def run_reference(a) -> int:
-    """The reference path on the host cores: its C++ needs Eigen (absent) and
-    cuSOLVER/cuFFT, so the CPU path timed is the oracle port, all threads."""
+    """The reference path on the host cores, timed on whole clips.  Its C++
+    needs Eigen (absent) and cuSOLVER/cuFFT, so the CPU path timed is the
+    oracle port on all threads.  One step = one clip of the workload (its own
+    seeded mask); W untimed clips, then K timed clips."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    vals = []
+    times = []
     for i in range(a.warmup + a.steps):
-        s = cpu_sample()
+        t, _ = cpu_clip(seed=10_000 + i)
         if i >= a.warmup:
-            vals.append(s["value"])
-    v = statistics.median(vals)
+            times.append(t)
+    total = sum(times)
+    v = len(times) / total
+    cpu = {"value": v, "unit": "clips/s", "cores": _cpu_threads(), "kind": "port",
+           "sample": _clip_sample_text(6, 200) + "; %d timed clips, %.2f s each (median)"
+           % (len(times), statistics.median(times))}
     out = {"impl": "reference", "metric": METRIC, "value": v, "unit": "clips/s", "n_gpus": a.gpus,
-           "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1000.0 * CLIPS / v,
+           "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1000.0 * total / len(times),
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-           "data": "synthetic (seeded lines+contacts masks)",
-           "config": {"workload": WORKLOAD, "clips_per_step": CLIPS, "path": "CPU oracle port"},
-           "cpu_baseline": dict(s, value=v),
+           "data": "synthetic (seeded lines+contacts masks, 36% absorber)",
+           "config": {"workload": WORKLOAD, "clips_per_step": 1, "precision": "fp64",
+                      "path": "CPU oracle port, whole clips"},
+           "cpu_baseline": cpu,
            "e2e": {"value": v, "unit": "clips/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
     return 0
+
+
+LAT_REPLAYS = 200
+PLAIN_REPEATS = 3
+
+
+def _percentile(sorted_vals, q: float) -> float:
+    """Nearest-rank percentile of an ascending list."""
+    n = len(sorted_vals)
+    i = max(0, min(n - 1, int(math.ceil(q * n)) - 1))
+    return sorted_vals[i]
 
 
 # ---------------------------------------------------------------- ranks
@@ -170,72 +176,79 @@ def _measured_peaks():
         return None
 
 
-def _with_measured_peaks(out: dict, achieved: float) -> dict:
-    """Adds the measured-peaks file and the fraction of its dense bf16 rate (the
-    file's only tensor figure; a TF32 kernel's own bound is the in-run TF32 rate)."""
+FALLBACK_BF16_TFLOPS = 1590.0  # dense bf16 GEMM measured earlier on this GPU type
+
+
+def _bf16_peak():
+    """(peak TFLOP/s, source): the measured dense bf16 burst rate of the
+    measured-peaks file (the kernel is timed alone), else the fallback figure."""
     mp = _measured_peaks()
-    if mp is not None:
-        out["measured_peaks_file"] = mp
-        bf = mp.get("bf16_tflops")
-        if isinstance(bf, (int, float)) and bf > 0:
-            out["frac_of_measured_bf16"] = achieved / float(bf)
-    return out
+    bf = mp.get("bf16_tflops") if mp else None
+    if isinstance(bf, (int, float)) and bf > 0:
+        return float(bf), "of measured (MEASURED_PEAKS.json bf16_tflops, burst)", mp
+    return FALLBACK_BF16_TFLOPS, "of fallback (no measured-peaks file)", None
 
 
 def dominant_kernel_roofline(plan, U, precision, dev, stream, L):
     """Roofline of the step's dominant kernel at the pipeline's shape (all U
     units of N orders), timed live with CUDA events on the launching stream.
 
-    mixed: the tcgen05 TF32x3 complex GEMM; algorithmic work = 24*N^3 TF32
-    FLOP per unit (3 split products x 4 real products x 2N^3), peak = cuBLAS
-    TF32 GEMM measured in this run.  fp64: the DMMA complex GEMM, 8*N^3 FLOP
-    per unit, peak = cuBLAS ZGEMM measured in this run (the pool's measured
-    peaks cover BF16 and HBM only)."""
+    Algorithmic work: one complex N x N x N product = 8 N^3 real FLOP per unit
+    (the convention for a complex GEMM, whatever the arithmetic that carries
+    it out); peak = the measured dense bf16 tensor rate.  Secondary keys give
+    the rate the kernel actually executes: mixed = TF32x3, three TF32 products
+    per real product (24 N^3 TF32 FLOP per unit) against a cuBLAS TF32 GEMM
+    measured in this run; fp64 = DMMA against cuBLAS ZGEMM measured here."""
     import torch
     N = plan.orders.n
     A = torch.randn(U, N, N, dtype=torch.complex128, device=dev)
     B = torch.randn(U, N, N, dtype=torch.complex128, device=dev)
     C = torch.empty_like(A)
     s = stream.cuda_stream
+    flop = 8.0 * N ** 3 * U
     if precision == "mixed":
         wb = L.lib().euv_zgemm_tf32x3_workspace_bytes(N, N, N, U)
-        ws = torch.empty(wb, dtype=torch.uint8, device=dev)
+        ws = torch.empty(max(wb, 256), dtype=torch.uint8, device=dev)
 
         def gemm():
             L.call("euv_zgemm_tf32x3", N, N, N, L.c64(1, 0), None, A.data_ptr(), N, N * N,
                    B.data_ptr(), N, N * N, L.c64(0, 0), C.data_ptr(), N, N * N, L.c64(0, 0), U,
                    None, 0, ws.data_ptr(), wb, None, s)
-        flop = 24.0 * N ** 3 * U
-        ms = _time_ms(gemm, stream, 5)
+        ms = _time_ms(gemm, stream, 10)
         X = torch.randn(8192, 8192, dtype=torch.float32, device=dev)
         Y = torch.randn(8192, 8192, dtype=torch.float32, device=dev)
         old = torch.backends.cuda.matmul.allow_tf32
         torch.backends.cuda.matmul.allow_tf32 = True
-        peak = 2.0 * 8192 ** 3 / (_time_ms(lambda: torch.matmul(X, Y), stream, 5) / 1e3) / 1e12
+        tf32 = 2.0 * 8192 ** 3 / (_time_ms(lambda: torch.matmul(X, Y), stream, 5) / 1e3) / 1e12
         torch.backends.cuda.matmul.allow_tf32 = old
+        executed = 24.0 * N ** 3 * U / (ms / 1e3) / 1e12
         out = {"bound": "tensor",
-               "kernel": "gemm_tf32x3_kernel (tcgen05 kind::tf32, TMA, TMEM) incl. operand split, "
-                         "batch %d x %d^3 complex" % (U, N),
-               "peak_source": "cuBLAS TF32 GEMM 8192^3 (torch.matmul float32, allow_tf32) measured "
-                              "in this run",
-               "complex_fp64_equivalent_tflops": 8.0 * N ** 3 * U / (ms / 1e3) / 1e12,
-               "traffic": _traffic("gemm_tf32x3_n961.json")}
+               "kernel": "gemm_tf32x3_kernel (tcgen05 kind::tf32, TMEM accumulators), batch "
+                         "%d x %d^3 complex" % (U, N),
+               "traffic": _traffic("gemm_tf32x3_n961.json"),
+               "tf32x3_executed_tflops": executed,
+               "cublas_tf32_tflops_in_run": tf32,
+               "frac_of_cublas_tf32": executed / tf32}
     else:
         def gemm():
             L.call("euv_zgemm", N, N, N, L.c64(1, 0), None, A.data_ptr(), N, N * N, B.data_ptr(),
                    N, N * N, L.c64(0, 0), C.data_ptr(), N, N * N, L.c64(0, 0), U, None, 0, s)
-        flop = 8.0 * N ** 3 * U
         ms = _time_ms(gemm, stream, 5)
         X = torch.randn(4096, 4096, dtype=torch.complex128, device=dev)
         Y = torch.randn(4096, 4096, dtype=torch.complex128, device=dev)
-        peak = 8.0 * 4096 ** 3 / (_time_ms(lambda: torch.matmul(X, Y), stream, 3) / 1e3) / 1e12
+        zg = 8.0 * 4096 ** 3 / (_time_ms(lambda: torch.matmul(X, Y), stream, 3) / 1e3) / 1e12
         out = {"bound": "tensor", "kernel": "zgemm_kernel (DMMA m8n8k4 f64), batch %d x %d^3" % (U, N),
-               "peak_source": "cuBLAS ZGEMM 4096^3 (torch.matmul complex128) measured in this run",
-               "traffic": _traffic("zgemm_n961.json")}
+               "traffic": _traffic("zgemm_n961.json"),
+               "cublas_zgemm_tflops_in_run": zg}
+        out["frac_of_cublas_zgemm"] = flop / (ms / 1e3) / 1e12 / zg
     achieved = flop / (ms / 1e3) / 1e12
+    peak, src, mp = _bf16_peak()
     out.update({"achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                "ms_per_launch": ms, "algorithmic_flop_per_launch": flop})
-    return _with_measured_peaks(out, achieved)
+                "peak_source": src, "ms_per_launch": ms, "algorithmic_flop_per_launch": flop,
+                "algorithmic_model": "8*N^3 real FLOP per complex N^3 product x %d units" % U})
+    if mp is not None:
+        out["measured_peaks_file"] = mp
+    return out
 
 
 def library_path_sample(plan, masks_dev, dev, units_per_clip: int, n_src_images: int):
@@ -417,13 +430,21 @@ def main() -> int:
     torch.cuda.synchronize()
     barrier()
     clk = clocks.stop()
-    step_ms = [ev[i].elapsed_time(ev[i + 1]) for i in range(a.steps)]
     total_ms = max_over_ranks(ev[0].elapsed_time(ev[-1]))
     ms_per_step = total_ms / a.steps
     value = whole_job_rate(CLIPS, world, total_ms / a.steps)
-    lat = sorted(step_ms)
-    p50 = lat[len(lat) // 2]
-    p99 = lat[min(len(lat) - 1, int(round(0.99 * (len(lat) - 1))))]
+
+    # ---- step latency distribution: LAT_REPLAYS replays, each between two events
+    lev = [torch.cuda.Event(enable_timing=True) for _ in range(LAT_REPLAYS + 1)]
+    torch.cuda.synchronize()
+    lev[0].record(stream)
+    for i in range(LAT_REPLAYS):
+        b.replay()
+        lev[i + 1].record(stream)
+    torch.cuda.synchronize()
+    lat = sorted(lev[i].elapsed_time(lev[i + 1]) for i in range(LAT_REPLAYS))
+    p50 = _percentile(lat, 0.50)
+    p99 = _percentile(lat, 0.99)
 
     # ---- end to end through the public API: pinned host masks in, images out
     hin = torch.from_numpy(host).pin_memory()
@@ -455,13 +476,53 @@ def main() -> int:
     b.replay()
     torch.cuda.synchronize()
     intensity_err = float((b.image - img64).abs().max() / img64.abs().max())
-    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    p0.record(stream)
-    pb.run_plain()
-    p1.record(stream)
-    torch.cuda.synchronize()
-    plain_ms = max_over_ranks(p0.elapsed_time(p1))
+    plain_runs = []
+    for _ in range(PLAIN_REPEATS):
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        pb.run_plain()
+        p1.record(stream)
+        torch.cuda.synchronize()
+        plain_runs.append(p0.elapsed_time(p1))
+    plain_ms = max_over_ranks(statistics.median(plain_runs))
     plain_value = CLIPS * world / (plain_ms / 1000.0)
+    # the batched FP64 form under its own CUDA graph (same clips), for reference
+    fp64_batched = None
+    if a.precision == "mixed":
+        pb.run()
+        torch.cuda.synchronize()
+        pb.capture()
+        pb.replay()
+        q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        q0.record(stream)
+        for _ in range(PLAIN_REPEATS):
+            pb.replay()
+        q1.record(stream)
+        torch.cuda.synchronize()
+        fb_ms = max_over_ranks(q0.elapsed_time(q1) / PLAIN_REPEATS)
+        fp64_batched = {"value": CLIPS * world / (fb_ms / 1000.0), "unit": "clips/s",
+                        "ms_per_step": fb_ms, "what": "all 24 units per ampS launch, CUDA graph"}
+        pb.graph = None
+
+    # ---- the oracle on clip 0 of this rank's step: CPU baseline (whole clip,
+    # timed) and the error of both GPU forms against it
+    cpu, err_oracle = None, None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        try:
+            t_clip, ref = cpu_clip(rank_seeds(rank, CLIPS)[0])
+            cpu = {"value": 1.0 / t_clip, "unit": "clips/s", "cores": _cpu_threads(),
+                   "kind": "port", "sample": _clip_sample_text(b.U // CLIPS, plan.sdivsum) +
+                   "; %.2f s for the clip (clip 0 of the GPU step)" % t_clip}
+            err_oracle = {}
+            for name, im in (("mixed" if a.precision == "mixed" else "fp64", b.image),
+                             ("fp64", img64)):
+                e = 0.0
+                for p, pol in enumerate(("X", "Y")):
+                    r = torch.from_numpy(ref[pol]).to(dev)
+                    e = max(e, float((im[0, p] - r).abs().max() / r.abs().max()))
+                err_oracle[name] = e
+        except Exception as e:  # the baseline is reported, never required
+            cpu = {"error": repr(e)}
 
     roofline = dominant_kernel_roofline(plan, b.U, a.precision, dev, stream, L)
 
@@ -471,13 +532,6 @@ def main() -> int:
             libpath = library_path_sample(plan, b.masks, dev, b.U // CLIPS, plan.sdivsum * 2)
         except Exception as e:  # the baseline is reported, never required
             libpath = {"error": repr(e)}
-
-    cpu = None
-    if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        try:
-            cpu = cpu_sample()
-        except Exception as e:  # the baseline is reported, never required
-            cpu = {"error": repr(e)}
 
     out = {
         "metric": METRIC, "value": value, "unit": "clips/s", "n_gpus": world, "steps": a.steps,
@@ -491,9 +545,15 @@ def main() -> int:
                          % (b.work.numel() / 1e9),
                    "parallelism": "replicas x%d" % world, "cuda_graph": True},
         "p50_ms": p50, "p99_ms": p99,
-        "plain_fp64": {"value": plain_value, "unit": "clips/s", "ms_per_step": plain_ms},
+        "latency": {"replays": LAT_REPLAYS, "p50_ms": p50, "p99_ms": p99, "max_ms": lat[-1],
+                    "what": "one CUDA-graph replay of a 4-clip step, CUDA events"},
+        "plain_fp64": {"value": plain_value, "unit": "clips/s", "ms_per_step": plain_ms,
+                       "runs": PLAIN_REPEATS, "what": "one unit per ampS call, no graph (median)"},
         "speedup_vs_plain": value / plain_value,
+        "fp64_batched": fp64_batched,
+        "speedup_vs_fp64_batched": (value / fp64_batched["value"]) if fp64_batched else None,
         "intensity_err_vs_fp64": intensity_err,
+        "intensity_err_vs_oracle": err_oracle,
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
         "library_path_fp64": libpath,
         "gpu_launches": int(launches_per_step * a.steps),

@@ -409,7 +409,10 @@ int euv_lu_solve(int n, int nrhs, const euv_c64* d_lu, int lda, long long stride
 /* Matrix functions of a slice: for each b, C[b] = cos(sqrt(D) d[b]) and
  * S[b] = sin(sqrt(D) d[b]) / sqrt(D), by Taylor series and double-angle steps.
  * The outputs of absorberS0 / absorberS depend on their eigen-decomposition
- * D = W diag(al^2) W^-1 only through these two entire functions of D. */
+ * D = W diag(al^2) W^-1 only through these two entire functions of D.
+ * At most m_max double-angle steps are taken; a matrix whose norm asks for
+ * more gets m_max, and this call reports that nowhere (euv_amp reports it as
+ * EUV_STATUS_STEPS_CLAMPED): choose m_max with 2^m_max >= ||D||_1 d^2. */
 size_t euv_matfun_workspace_bytes(int n, int batch);
 int euv_matfun_cs(int n, const euv_c64* d_d, const double* d_thick, euv_c64* d_cos,
                   euv_c64* d_sin, int batch, int m_max, int precision, void* d_work,
@@ -418,12 +421,12 @@ int euv_matfun_cs(int n, const euv_c64* d_d, const double* d_thick, euv_c64* d_c
 /* Same as euv_matfun_cs (FP64), but without a workspace: no counterpart in
  * the reference, which allocates on every call.
  *
- * For callers that cannot allocate device memory: code that runs while a
- * framework captures a CUDA graph and forbids allocation inside the capture,
- * plug-ins whose host application owns all device memory through its own
- * allocator, and latency-critical loops that must not call cudaMalloc/cudaFree
- * because those calls can synchronise the whole device.  The caller passes
- * only the inputs and outputs; the scratch space is a fixed array of
+ * For callers that cannot allocate device memory: plug-ins whose host
+ * application owns all device memory through its own allocator and hands out
+ * none for scratch, hosts with a fixed device-memory budget set at start-up,
+ * and latency-critical loops that must not call cudaMalloc/cudaFree because
+ * those calls can synchronise the whole device.  The caller passes only the
+ * inputs and outputs; the scratch space is a fixed array of
  * EUV_NOALLOC_SCRATCH_BYTES (16 MiB) inside the library, resident on every GPU
  * that loads it until the process exits.  The function calls no allocator.
  *
@@ -432,7 +435,13 @@ int euv_matfun_cs(int n, const euv_c64* d_d, const double* d_thick, euv_c64* d_c
  *    EUV_ERR_BAD_ARG with a message and launch nothing.
  *  - The first call on each device looks up the array's device address
  *    (cudaGetSymbolAddress, with that device current); make that first call
- *    before any stream capture.
+ *    before any stream capture.  The address is kept for the life of the
+ *    process: after cudaDeviceReset (or any teardown of the device's primary
+ *    context) it is stale, so do not call this entry point after a reset.
+ *  - As in euv_matfun_cs, the double-angle steps are capped at m_max and a
+ *    call that needed more is not reported (no status word): pass an m_max
+ *    with 2^m_max >= ||D||_1 * max(d)^2 (about 8 covers an absorber slice of
+ *    tens of nm).
  *  - All calls share the one array and it keeps the last call's contents (the
  *    function clears what must start at zero).  Calls whose GPU work overlaps,
  *    e.g. on two streams at once, race on it: order them on one stream or

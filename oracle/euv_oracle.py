@@ -690,7 +690,56 @@ def rotate_many(k, MX, MY, px, py, sx0, sy0) -> np.ndarray:
 def abbe_family_fields(cfg: SimConfig, polar, Ax, lidx, midx, nsx, nsy, ndivs, pts,
                        linput, minput, z):
     """Pupil-grid fields of one family's source points (intensity.cpp:248-366).
-    Returns a list of (Fx, Fy, Fz) XDIV x YDIV spectra, one per source point."""
+    Returns a list of (Fx, Fy, Fz) XDIV x YDIV spectra, one per source point.
+
+    The reference loops over source points and, inside, over pupil points
+    (intensity.cpp:276-331, 333-366); the pupil loop is written here as array
+    operations on all pupil points of a source at once (same arithmetic per
+    point: the NA test, the order lookup, rotate(), E = ik R A and the phase)."""
+    k, dx, dy = cfg.k, cfg.dx, cfg.dy
+    MX, MY, NA = cfg.mx, cfg.my, cfg.na
+    kx0, ky0 = cfg.kx0, cfg.ky0
+    sx0 = 2.0 * PI / dx * nsx / float(ndivs) + kx0
+    sy0 = 2.0 * PI / dy * nsy / float(ndivs) + ky0
+    XD, YD = cfg.xdiv, cfg.ydiv
+    pos = {(int(a), int(b)): i for i, (a, b) in enumerate(zip(lidx, midx))}
+    z0 = cfg.z0
+    lin = np.asarray(linput, np.int64)
+    mn = np.asarray(minput, np.int64)
+    px_all = (lin + XD) % XD
+    py_all = (mn + YD) % YD
+    out = []
+    for (l0, m0) in pts:
+        kx = sx0 + 2.0 * PI / dx * l0
+        ky = sy0 + 2.0 * PI / dy * m0
+        F = np.zeros((3, XD, YD), np.complex128)
+        kxn = 2.0 * PI / dx * nsx / float(ndivs) + 2.0 * PI / dx * l0 + 2.0 * PI * lin / dx
+        kyn = 2.0 * PI / dy * nsy / float(ndivs) + 2.0 * PI / dy * m0 + 2.0 * PI * mn / dy
+        inside = (MX * MX * kxn * kxn + MY * MY * kyn * kyn) <= (NA * k) ** 2
+        sel = np.nonzero(inside)[0]
+        if sel.size:
+            try:
+                n = np.array([pos[(int(l0 + lin[i]), int(m0 + mn[i]))] for i in sel])
+            except KeyError:
+                raise ValueError("pupil order outside the order set")
+            a = Ax[(l0, m0)][n]
+            R = rotate_many(k, MX, MY, kxn[sel], kyn[sel], kx0, ky0)      # [n, 3, 2]
+            if polar == "X":
+                E = 1j * k * (R[:, :, 0] * (a / np.sqrt(k * k - kx * kx))[:, None])
+            else:
+                E = 1j * k * (R[:, :, 1] * (a / np.sqrt(k * k - ky * ky))[:, None])
+            phase = np.exp(1j * ((kxn[sel] + kx0) ** 2 + (kyn[sel] + ky0) ** 2) / 2.0 / k * z0
+                           + 1j * (MX * MX * kxn[sel] ** 2 + MY * MY * kyn[sel] ** 2) / 2.0 / k
+                           * float(z))
+            F[:, px_all[sel], py_all[sel]] = (E * phase[:, None]).T
+        out.append(F)
+    return out
+
+
+def _abbe_family_fields_loop(cfg: SimConfig, polar, Ax, lidx, midx, nsx, nsy, ndivs, pts,
+                             linput, minput, z):
+    """The same fields with the reference's pupil loop written out point by
+    point (intensity.cpp:276-366): the check of the array form."""
     k, dx, dy = cfg.k, cfg.dx, cfg.dy
     MX, MY, NA = cfg.mx, cfg.my, cfg.na
     kx0, ky0 = cfg.kx0, cfg.ky0

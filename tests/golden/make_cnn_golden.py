@@ -48,7 +48,8 @@ def synthetic_raster(seed: int = 3) -> np.ndarray:
 
 
 def main() -> int:
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    from refroot import reference_root
+    ref = reference_root()
     d = os.path.join(ref, "cnn", "cnn", "predict")
     pl = types.ModuleType("pytorch_lightning")
     pl.LightningModule = torch.nn.Module

@@ -23,7 +23,8 @@ FILES = {
 
 
 def main() -> int:
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    from refroot import reference_root
+    root = reference_root()
     here = os.path.dirname(os.path.abspath(__file__))
     for src, dst in FILES.items():
         with open(os.path.join(root, src), "rb") as fh:

@@ -61,7 +61,8 @@ def uniform_amplitudes():
 
 
 def main() -> int:
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    from refroot import reference_root
+    ref = reference_root()
     lin_dir = os.path.join(ref, "cnn", "intensity", "linear")
     _install_stand_ins()
     sys.path.insert(0, lin_dir)

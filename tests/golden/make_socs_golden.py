@@ -55,7 +55,8 @@ def _install_stand_ins() -> None:
 
 def main() -> int:
     from make_linear_golden import uniform_amplitudes
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    from refroot import reference_root
+    ref = reference_root()
     d = os.path.join(ref, "cnn", "intensity", "stccsocs")
     _install_stand_ins()
     sys.path.insert(0, d)

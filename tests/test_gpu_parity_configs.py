@@ -1,0 +1,181 @@
+"""The CUDA path against the FP64 oracle at the configurations that are measured.
+
+* batched (the bench workload): 1024 nm clip, NA 0.55 4x/8x, 31x31 = 961
+  orders, 200-point annular source in 3 Bloch families, X and Y polarisation:
+  every unit's amplitudes Ax, both images, and the M3D parameters;
+* large: 2048 nm clip, 41x41 = 1681 orders, 8 sidewall slices of 7.5 nm, one
+  Bloch family of 380 source points: amplitudes and images with the bottom
+  slice's sigma for every slice (the reference), amplitudes with each slice's
+  own sigma;
+* serving shape: a 2048 nm clip with 41x41 orders and one slice, as the server
+  builds it for a request of 120 source points.
+
+Bars (max |x - x_ref| / max |x_ref| per output array): the FP64 form 1e-8
+(the oracle is eigen-based, the library eigen-free: agreement to rounding of
+two algorithms); the mixed form 1e-4 (the north-star intensity bar, applied to
+the amplitudes too).  M3D slopes (ax, ay) can vanish on a clip, so the mixed
+form's M3D errors are measured against max |a0|.  The errors are printed, so
+that a run with ``-s`` lists them per configuration."""
+import numpy as np
+import pytest
+
+from euvlitho_b200.config import preset
+from oracle import euv_oracle as O
+from tests.helpers import flat_bits, packed, random_mask, rel_err, to_oracle
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-8
+MIXED_TOL = 1e-4
+
+
+def _sidewall(cfg, seed):
+    """Per-slice masks (slice 0 = top): the absorber eroded by one more pixel
+    on every edge from the bottom slice upward, every other slice."""
+    m = random_mask(cfg.ndivx, cfg.ndivy, seed=seed)
+    out = []
+    for n in range(cfg.nabs):
+        e = m.copy()
+        for _ in range((cfg.nabs - 1 - n) // 2):
+            # absorber = 0: a max over the cross grows the vacuum (erodes the absorber)
+            e = np.maximum.reduce([e, np.roll(e, 1, 0), np.roll(e, -1, 0), np.roll(e, 1, 1),
+                                   np.roll(e, -1, 1)])
+        out.append(e)
+    return out
+
+
+def _batch_ax(plan, b):
+    """{(pol, nsx, nsy): {source order: Ax column}} of clip 0 from a run batch."""
+    ax = b.ax.cpu().numpy()
+    out = {}
+    t = 0
+    for pol in plan.pols:
+        for f in plan.fams:
+            out[(pol, f.nsx, f.nsy)] = {pt: ax[t, s] for s, pt in enumerate(f.pts)}
+            t += 1
+    return out
+
+
+def _run_clip(cfg, masks, precision, pols=("X", "Y")):
+    import torch
+    from euvlitho_b200.engine import Plan
+    plan = Plan(cfg, device=torch.device("cuda", 0), pols=pols, precision=precision)
+    m = plan.as_mask_tensor(torch.from_numpy(masks))
+    b = plan.intensity_batch(m.shape[0], m.shape[1])
+    b.masks.copy_(m)
+    b.run()
+    b.check()
+    img = b.image.cpu().numpy()
+    return plan, img, _batch_ax(plan, b)
+
+
+def _compare(name, plan, img, ax, ref_img, ref_ax, tol):
+    worst_ax = 0.0
+    for key, cols in ax.items():
+        for pt, v in cols.items():
+            worst_ax = max(worst_ax, rel_err(v, ref_ax[key][pt]))
+    worst_img = max(rel_err(img[0, p], ref_img[pol]) for p, pol in enumerate(plan.pols))
+    print("%s: Ax max rel err %.2e, image %.2e" % (name, worst_ax, worst_img))
+    assert worst_ax < tol, (name, "Ax", worst_ax)
+    assert worst_img < tol, (name, "image", worst_img)
+
+
+# ---------------------------------------------------------------- batched (N = 961)
+@pytest.fixture(scope="module")
+def batched_ref():
+    cfg = preset("batched")
+    m = random_mask(cfg.ndivx, cfg.ndivy, seed=2024)
+    img, ax = O.intensity(to_oracle(cfg), flat_bits(m), polars=("X", "Y"), return_ax=True)
+    return cfg, m, img, ax
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", FP64_TOL), ("mixed", MIXED_TOL)])
+def test_batched_clip_matches_oracle(cuda, batched_ref, precision, tol):
+    cfg, m, ref_img, ref_ax = batched_ref
+    plan, img, ax = _run_clip(cfg, packed(m)[None, None], precision)
+    assert plan.orders.n == 961 and len(plan.fams) == 3 and plan.sdivsum == 200
+    _compare("batched %s" % precision, plan, img, ax, ref_img, ref_ax, tol)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batched_m3d_matches_oracle(cuda, precision):
+    import torch
+    from euvlitho_b200.engine import Plan
+    cfg = preset("batched")
+    m = random_mask(cfg.ndivx, cfg.ndivy, seed=2025)
+    plan = Plan(cfg, device=cuda, pols=("X",), precision=precision)
+    res = plan.m3d(torch.from_numpy(packed(m)[None]))
+    ref = O.m3d(to_oracle(cfg), flat_bits(m))
+    xin = plan.xinput == 1
+    assert np.array_equal(ref["xinput"], plan.xinput)
+    scale = np.max(np.abs(ref["a0"]))
+    errs = {"a0": np.max(np.abs(res["a0"][0].cpu().numpy() - ref["a0"])) / scale}
+    for k in ("ax", "ay"):
+        errs[k] = np.max(np.abs(res[k][0].cpu().numpy()[xin] - ref[k])) / scale
+    print("batched M3D %s (max abs err / max |a0|): " % precision +
+          ", ".join("%s %.2e" % kv for kv in errs.items()))
+    tol = FP64_TOL if precision == "fp64" else MIXED_TOL
+    for k, e in errs.items():
+        assert e < tol, (k, e)
+
+
+# ---------------------------------------------------------------- large (N = 1681, 8 slices)
+@pytest.fixture(scope="module")
+def large_ref():
+    cfg = preset("large")
+    sl = _sidewall(cfg, seed=77)
+    img, ax = O.intensity(to_oracle(cfg), [flat_bits(x) for x in sl], polars=("X", "Y"),
+                          return_ax=True)
+    return cfg, sl, img, ax
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", FP64_TOL), ("mixed", MIXED_TOL)])
+def test_large_sidewall_clip_matches_oracle(cuda, large_ref, precision, tol):
+    cfg, sl, ref_img, ref_ax = large_ref
+    masks = np.stack([packed(x) for x in sl])[None]
+    plan, img, ax = _run_clip(cfg, masks, precision)
+    assert plan.orders.n == 1681 and cfg.nabs == 8 and len(plan.fams) == 1
+    _compare("large %s" % precision, plan, img, ax, ref_img, ref_ax, tol)
+
+
+@pytest.fixture(scope="module")
+def large_refresh_ref():
+    cfg = preset("large").with_(refresh_sigma=True)
+    sl = _sidewall(cfg, seed=78)
+    oc = to_oracle(cfg)
+    L, M = cfg.order_limits()
+    li, mi = O.order_set(cfg.order_kind, L, M)
+    nd, fams = O.source(oc)
+    (nsx, nsy), pts = [(k, v) for k, v in fams.items() if v][0]
+    sx0 = 2 * O.PI / oc.dx * nsx / nd + oc.kx0
+    sy0 = 2 * O.PI / oc.dy * nsy / nd + oc.ky0
+    ax = O.amp_s("X", [flat_bits(x) for x in sl], oc, li, mi, L, M, sx0, sy0, source_orders=pts)
+    return cfg, sl, {("X", nsx, nsy): ax}
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", FP64_TOL), ("mixed", MIXED_TOL)])
+def test_large_sidewall_own_sigma_amplitudes(cuda, large_refresh_ref, precision, tol):
+    cfg, sl, ref_ax = large_refresh_ref
+    masks = np.stack([packed(x) for x in sl])[None]
+    plan, _, ax = _run_clip(cfg, masks, precision, pols=("X",))
+    worst = max(rel_err(v, ref_ax[key][pt]) for key, cols in ax.items() for pt, v in cols.items())
+    print("large, own sigma per slice, %s: Ax max rel err %.2e" % (precision, worst))
+    assert worst < tol
+
+
+# ---------------------------------------------------------------- serving shape 2048 nm / 41^2
+@pytest.fixture(scope="module")
+def serving_ref():
+    from euvlitho_b200.serving import ClipKey, config_for
+    cfg = config_for(ClipKey(period=2048, box=20, n_src=120))
+    m = random_mask(cfg.ndivx, cfg.ndivy, seed=4096)
+    img, ax = O.intensity(to_oracle(cfg), flat_bits(m), polars=("X", "Y"), return_ax=True)
+    return cfg, m, img, ax
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", FP64_TOL), ("mixed", MIXED_TOL)])
+def test_serving_shape_2048nm_41x41_matches_oracle(cuda, serving_ref, precision, tol):
+    cfg, m, ref_img, ref_ax = serving_ref
+    plan, img, ax = _run_clip(cfg, packed(m)[None, None], precision)
+    assert plan.orders.n == 1681 and plan.sdivsum == 120
+    _compare("serving 2048 nm 41x41 %s" % precision, plan, img, ax, ref_img, ref_ax, tol)

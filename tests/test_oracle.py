@@ -124,3 +124,28 @@ def test_pin_summary_within_print_precision():
     assert s["a0_max_abs_err_over_max"] < 4e-3
     assert s["ax_max_abs_err_over_max"] < 1e-3 and s["ay_max_abs_err_over_max"] < 1e-3
     assert s["a0_median_abs_err"] < 5e-6
+
+
+@pytest.mark.parametrize("pol", ["X", "Y"])
+def test_abbe_fields_array_form_equals_pupil_loop(pol):
+    """The oracle's Abbe fields, written as array operations over the pupil
+    points, equal the point-by-point loop of intensity.cpp:276-366."""
+    from euvlitho_b200.config import preset
+    from tests.helpers import to_oracle
+    cfg = preset("small")
+    oc = to_oracle(cfg)
+    m = flat_bits(random_mask(cfg.ndivx, cfg.ndivy, seed=5))
+    L, M = cfg.order_limits()
+    li, mi = O.order_set(cfg.order_kind, L, M)
+    nd, fams = O.source(oc)
+    lin, mn, _, _ = O.pupil_set(oc)
+    for (nsx, nsy), pts in fams.items():
+        if not pts:
+            continue
+        sx0 = 2 * O.PI / oc.dx * nsx / nd + oc.kx0
+        sy0 = 2 * O.PI / oc.dy * nsy / nd + oc.ky0
+        Ax = O.amp_s(pol, m, oc, li, mi, L, M, sx0, sy0, source_orders=pts)
+        a = O.abbe_family_fields(oc, pol, Ax, li, mi, nsx, nsy, nd, pts, lin, mn, 20)
+        b = O._abbe_family_fields_loop(oc, pol, Ax, li, mi, nsx, nsy, nd, pts, lin, mn, 20)
+        for x, y in zip(a, b):
+            assert np.max(np.abs(x - y)) <= 1e-13 * max(1.0, np.max(np.abs(y)))

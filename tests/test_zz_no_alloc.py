@@ -1,7 +1,7 @@
 """euv_matfun_cs_noalloc: the entry point for callers that cannot allocate
-device memory (graph-capturing frameworks that forbid allocation, plug-ins
-whose host owns the device memory, latency-critical loops that must avoid the
-device-wide synchronisation of cudaMalloc/cudaFree).  It uses a fixed 16 MiB
+device memory (plug-ins whose host owns all device memory, hosts with a fixed
+device-memory budget, latency-critical loops that must avoid the device-wide
+synchronisation of cudaMalloc/cudaFree).  It uses a fixed 16 MiB
 scratch array inside the library instead of a caller workspace.
 
 Checked through the C ABI against the workspace entry point euv_matfun_cs on
