@@ -40,7 +40,16 @@ EXPORTS = (
     "euv_heev_workspace_bytes", "euv_heev", "euv_socs_workspace_bytes", "euv_socs_image",
     "euv_cnn_blob_bytes", "euv_cnn_pack", "euv_cnn_workspace_bytes", "euv_cnn_predict",
     "euv_cnn_downsample",
+    "euv_config_reference", "euv_plan_create", "euv_plan_destroy", "euv_plan_get_info",
+    "euv_plan_get_orders", "euv_plan_get_pupil", "euv_plan_get_sources",
+    "euv_plan_get_na_sources", "euv_plan_get_abbe_table", "euv_plan_device_bytes",
+    "euv_plan_upload", "euv_plan_check", "euv_plan_intensity_workspace_bytes",
+    "euv_plan_intensity", "euv_plan_amp_workspace_bytes", "euv_plan_amp",
+    "euv_plan_m3d_workspace_bytes", "euv_plan_m3d",
 )
+EUV_ORDERS_DIAMOND = 0
+EUV_ORDERS_ELLIPSE = 1
+EUV_ORDERS_BOX = 2
 
 
 class EuvError(RuntimeError):
@@ -154,6 +163,30 @@ class CnnDesc(C.Structure):
     ]
 
 
+class Config(C.Structure):
+    """euv_config: the driver constants of intensity.cpp / m3d.cpp as parameters."""
+    _fields_ = [
+        ("ndivx", C.c_int), ("ndivy", C.c_int), ("delta", C.c_double),
+        ("wavelength", C.c_double), ("theta0", C.c_double), ("azimuth", C.c_double),
+        ("na", C.c_double), ("mx", C.c_int), ("my", C.c_int), ("illum_type", C.c_int),
+        ("sigma1", C.c_double), ("sigma2", C.c_double), ("openangle", C.c_double),
+        ("sigmadiv", C.c_double), ("ndivs", C.c_int), ("max_sources", C.c_int),
+        ("n_slices", C.c_int), ("eabs", c64 * EUV_MAX_SLICES),
+        ("dabs", C.c_double * EUV_MAX_SLICES), ("z0_offset", C.c_double), ("stack", Stack),
+        ("refresh_sigma", C.c_int), ("order_kind", C.c_int), ("cut", C.c_double),
+        ("lbox", C.c_int), ("mbox", C.c_int), ("z", C.c_double), ("yflip_offset", C.c_int),
+        ("n_pols", C.c_int), ("pols", C.c_int * 2), ("precision", C.c_int),
+    ]
+
+
+class PlanInfo(C.Structure):
+    _fields_ = [(n, C.c_int) for n in (
+        "n_orders", "lmax", "mmax", "ncut", "lpx", "lpy", "lsx", "lsy", "n_na_sources", "ndivs",
+        "n_families", "n_src_max", "sdivsum", "n_pols", "units_per_clip", "xdiv", "ydiv",
+        "fdivx", "fdivy", "n_orders_narrow")] + [
+        ("k", C.c_double), ("kx0", C.c_double), ("ky0", C.c_double), ("z0", C.c_double)]
+
+
 _lib: Optional[C.CDLL] = None
 
 
@@ -219,6 +252,37 @@ def _declare(lib: C.CDLL) -> None:
     lib.euv_cnn_predict.argtypes = [C.POINTER(CnnDesc), P, P, P, P, sz, P]
     lib.euv_cnn_downsample.restype = i
     lib.euv_cnn_downsample.argtypes = [i, P, P, P]
+    PP = C.POINTER(P)
+    lib.euv_config_reference.restype = None
+    lib.euv_config_reference.argtypes = [C.POINTER(Config)]
+    lib.euv_plan_create.restype = i
+    lib.euv_plan_create.argtypes = [C.POINTER(Config), PP]
+    lib.euv_plan_destroy.restype = None
+    lib.euv_plan_destroy.argtypes = [P]
+    lib.euv_plan_get_info.restype = i
+    lib.euv_plan_get_info.argtypes = [P, C.POINTER(PlanInfo)]
+    for fn, n in (("euv_plan_get_orders", 2), ("euv_plan_get_pupil", 3),
+                  ("euv_plan_get_sources", 5), ("euv_plan_get_na_sources", 2)):
+        getattr(lib, fn).restype = i
+        getattr(lib, fn).argtypes = [P] + [P] * n
+    lib.euv_plan_get_abbe_table.restype = i
+    lib.euv_plan_get_abbe_table.argtypes = [P, i, P, P]
+    lib.euv_plan_device_bytes.restype = sz
+    lib.euv_plan_device_bytes.argtypes = [P, i]
+    lib.euv_plan_upload.restype = i
+    lib.euv_plan_upload.argtypes = [P, i, P, sz, P]
+    lib.euv_plan_check.restype = i
+    lib.euv_plan_check.argtypes = [P, P, P]
+    for fn in ("euv_plan_intensity_workspace_bytes", "euv_plan_amp_workspace_bytes",
+               "euv_plan_m3d_workspace_bytes"):
+        getattr(lib, fn).restype = sz
+        getattr(lib, fn).argtypes = [P, i, i]
+    lib.euv_plan_intensity.restype = i
+    lib.euv_plan_intensity.argtypes = [P, P, i, i, P, P, sz, P]
+    lib.euv_plan_amp.restype = i
+    lib.euv_plan_amp.argtypes = [P, i, d, d, P, i, i, P, P, sz, P]
+    lib.euv_plan_m3d.restype = i
+    lib.euv_plan_m3d.argtypes = [P, P, i, i, P, P, P, P, sz, P]
 
 
 def lib() -> C.CDLL:
@@ -270,3 +334,35 @@ def check_status(where: str, bits: int) -> None:
         code = EUV_ERR_TIMEOUT if bits & EUV_STATUS_TIMEOUT else (
             EUV_ERR_SINGULAR if bits & EUV_STATUS_SINGULAR else EUV_ERR_CUDA)
         raise EuvError(where, code, "device status 0x%x: %s" % (int(bits), msg))
+
+
+_ORDER_KIND = {"diamond": EUV_ORDERS_DIAMOND, "ellipse": EUV_ORDERS_ELLIPSE, "box": EUV_ORDERS_BOX}
+
+
+def config_struct(cfg, pols=("X",), precision: int = EUV_PREC_FP64) -> Config:
+    """euv_config of a SimConfig (the same fields; permittivities as given)."""
+    c = Config()
+    c.ndivx, c.ndivy, c.delta, c.wavelength = cfg.ndivx, cfg.ndivy, cfg.delta, cfg.wavelength
+    c.theta0, c.azimuth, c.na, c.mx, c.my = cfg.theta0, cfg.azimuth, cfg.na, cfg.mx, cfg.my
+    c.illum_type, c.sigma1, c.sigma2 = cfg.illum_type, cfg.sigma1, cfg.sigma2
+    c.openangle, c.sigmadiv = cfg.openangle, cfg.sigmadiv
+    c.ndivs = 0 if cfg.ndivs is None else int(cfg.ndivs)
+    c.max_sources = 0 if cfg.max_sources is None else int(cfg.max_sources)
+    c.n_slices = cfg.nabs
+    for n in range(cfg.nabs):
+        c.eabs[n] = c64.of(cfg.eabs[n])
+        c.dabs[n] = float(cfg.dabs[n])
+    c.z0_offset = cfg.z0_offset
+    st = cfg.stack
+    c.stack = Stack(c64.of(st.n_mo ** 2), c64.of(st.n_si ** 2), c64.of(st.n_ru ** 2),
+                    c64.of(st.n_mosi2 ** 2), c64.of(st.n_rusi ** 2), c64.of(st.n_sio2 ** 2),
+                    st.d_mo, st.d_mosi, st.d_si, st.d_simo, st.d_siru, st.d_ru, st.nml)
+    c.refresh_sigma = 1 if cfg.refresh_sigma else 0
+    c.order_kind = _ORDER_KIND[cfg.order_kind]
+    c.cut, c.lbox, c.mbox, c.z = cfg.cut, cfg.lbox, cfg.mbox, float(cfg.z)
+    c.yflip_offset = cfg.yflip_offset
+    c.n_pols = len(pols)
+    for i, p in enumerate(pols):
+        c.pols[i] = {"X": 0, "Y": 1}[p]
+    c.precision = precision
+    return c

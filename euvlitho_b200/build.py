@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libeuvl_b200.so")
-SOURCES = ["api.cu", "zgemm.cu", "lu.cu", "rcwa.cu", "abbe.cu", "m3d.cu", "gemm_mixed.cu", "linear.cu", "raster.cu", "jacobi.cu", "socs.cu", "cnn.cu"]
+SOURCES = ["api.cu", "zgemm.cu", "lu.cu", "rcwa.cu", "abbe.cu", "m3d.cu", "gemm_mixed.cu", "linear.cu", "raster.cu", "jacobi.cu", "socs.cu", "cnn.cu", "plan.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

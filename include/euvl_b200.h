@@ -363,6 +363,131 @@ int euv_m3d_fit(const euv_m3d_desc* desc, const euv_c64* d_ax_wide, const euv_c6
                 euv_c64* d_a0, euv_c64* d_ax, euv_c64* d_ay, void* stream);
 
 /* ------------------------------------------------------------------------ */
+/* Plans: the configuration of the reference drivers and its tables, for C and
+ * C++ callers that port intensity.cpp / m3d.cpp onto the library without any
+ * other host code.
+ *
+ * euv_config holds the constants of intensity.cpp:44-146 / m3d.cpp:34-157 as
+ * parameters (euv_config_reference() fills the reference's values).  A plan
+ * builds, on the host, every table those drivers compute before their loops:
+ *   - the order set (rounded diamond intensity.cpp:148-164, ellipse
+ *     m3d.cpp:113-129, or an explicit box), l outer / m inner;
+ *   - the pupil set with the xinput flag (intensity.cpp:166-195,
+ *     m3d.cpp:160-195), l-major;
+ *   - the Bloch families and their source orders (source(),
+ *     intensity.cpp:467-502; max_sources keeps the first points);
+ *   - per (polarisation, family, source, pupil point) the E-field factor
+ *     i k R(.) / sqrt(k^2 - k_s^2) * phase of rotate() and the pupil phase
+ *     with defocus (intensity.cpp:276-353, 423-465), and the order index the
+ *     point reads (the tables euv_abbe takes);
+ *   - the NA-circle source orders of ampS (header.h:1394-1397), the narrow
+ *     order set of m3d.cpp:101-129 and the (pupil point, source) -> order
+ *     pairs of the M3D fit (m3d.cpp:426-450).
+ * euv_plan_create allocates host memory only; euv_plan_upload copies the
+ * tables into caller device memory (euv_plan_device_bytes), sized for up to
+ * max_clips clips per call, after which the run functions can be called.
+ * A plan is read-only after upload except for the M3D narrow solves, which
+ * the first euv_plan_m3d call computes into the plan's device tables: make
+ * that first call before sharing the plan between streams.  Plans on
+ * different devices need their own upload. */
+#define EUV_ORDERS_DIAMOND 0
+#define EUV_ORDERS_ELLIPSE 1
+#define EUV_ORDERS_BOX 2
+
+typedef struct {
+  int ndivx, ndivy;        /* clip on the mask grid (pixels of 1 nm: dx = ndivx nm) */
+  double delta;            /* Fourier-grid pixel (nm): fdivx = ndivx / delta */
+  double wavelength;       /* nm */
+  double theta0, azimuth;  /* chief ray (deg): kx0 = k sin(theta0) cos(90 - azimuth) */
+  double na;
+  int mx, my;              /* demagnification (anamorphic: my = 8) */
+  int illum_type;          /* 0 conventional, 1 annular, 2 X dipole, 3 Y dipole */
+  double sigma1, sigma2, openangle, sigmadiv;
+  int ndivs;               /* Bloch families per axis; <= 0: the reference's rule */
+  int max_sources;         /* keep the first max_sources source points; <= 0: all */
+  int n_slices;            /* absorber slices (slice 0 = top) */
+  euv_c64 eabs[EUV_MAX_SLICES]; /* permittivity of each slice */
+  double dabs[EUV_MAX_SLICES];  /* thickness of each slice (nm) */
+  double z0_offset;        /* z0 = sum(dabs) + z0_offset (intensity.cpp:80) */
+  euv_stack stack;
+  int refresh_sigma;       /* 0: the bottom slice's sigma for every slice (reference) */
+  int order_kind;          /* EUV_ORDERS_* */
+  double cut;              /* order cut of the diamond / ellipse sets */
+  int lbox, mbox;          /* half sizes of the box set */
+  double z;                /* defocus (nm) */
+  int yflip_offset;        /* as in euv_mask_spectrum */
+  int n_pols;              /* 1 or 2 */
+  int pols[2];             /* 0 = X, 1 = Y */
+  int precision;           /* EUV_PREC_FP64 or EUV_PREC_MIXED */
+} euv_config;
+
+typedef struct {
+  int n_orders, lmax, mmax;   /* order set and its limits (LMAX, MMAX) */
+  int ncut, lpx, lpy;         /* pupil points and the pupil box half sizes */
+  int lsx, lsy;               /* lsmaxX, lsmaxY */
+  int n_na_sources;           /* NA-circle source orders of ampS */
+  int ndivs, n_families, n_src_max, sdivsum;
+  int n_pols, units_per_clip; /* units = families x polarisations */
+  int xdiv, ydiv, fdivx, fdivy;
+  int n_orders_narrow;        /* m3d.cpp narrow set (ellipse, cut 1.5) */
+  double k, kx0, ky0, z0;
+} euv_plan_info;
+
+typedef struct euv_plan euv_plan;
+
+/* The reference configuration (intensity.cpp:44-146, header.h:1217-1230):
+ * NA 0.33, 4x, 2048 nm, annular 0.55-0.9, Ta 60 nm, X polarisation, FP64. */
+void euv_config_reference(euv_config* cfg);
+/* Host tables of cfg; *plan is freed by euv_plan_destroy.  EUV_ERR_BAD_ARG
+ * for an invalid configuration (e.g. an order set that misses a diffracted
+ * order the Abbe loop reads, or reaches evanescent orders: header.h:1283
+ * takes a real square root). */
+int euv_plan_create(const euv_config* cfg, euv_plan** plan);
+void euv_plan_destroy(euv_plan* plan);
+int euv_plan_get_info(const euv_plan* plan, euv_plan_info* info);
+/* Host copies of the tables (caller arrays of the sizes in euv_plan_info):
+ * orders l, m [n_orders]; pupil l, m, xinput [ncut]; family nsx, nsy, count
+ * [n_families] and source orders l, m [sdivsum] family by family; the NA
+ * sources l, m [n_na_sources]; Abbe table t = pol_index * n_families + family:
+ * coef [n_src_max][ncut][3], nidx [n_src_max][ncut].  NULL arrays are skipped. */
+int euv_plan_get_orders(const euv_plan* plan, int* h_l, int* h_m);
+int euv_plan_get_pupil(const euv_plan* plan, int* h_l, int* h_m, int* h_xinput);
+int euv_plan_get_sources(const euv_plan* plan, int* h_nsx, int* h_nsy, int* h_count, int* h_l,
+                         int* h_m);
+int euv_plan_get_na_sources(const euv_plan* plan, int* h_l, int* h_m);
+int euv_plan_get_abbe_table(const euv_plan* plan, int t, euv_c64* h_coef, int* h_nidx);
+/* Device tables for up to max_clips clips per call. */
+size_t euv_plan_device_bytes(const euv_plan* plan, int max_clips);
+int euv_plan_upload(euv_plan* plan, int max_clips, void* d_tables, size_t bytes, void* stream);
+/* Reads and clears the plan's device status word (synchronises the stream):
+ * EUV_ERR_TIMEOUT / EUV_ERR_SINGULAR if a run since the last check reported
+ * one (EUV_STATUS_* bits in *bits), else EUV_OK. */
+int euv_plan_check(const euv_plan* plan, int* bits, void* stream);
+
+/* The Abbe images of n_clips clips (intensity.cpp:219-408 for every
+ * polarisation of the plan): d_masks [clip][n_mask_slices][ndivx*ndivy/8]
+ * mask.bin bits (n_mask_slices 1 = one mask for all slices, the reference;
+ * or one per slice); d_image [clip][pol][xdiv][ydiv], I[x][y], overwritten.
+ * One batched ampS of all (clip, family, polarisation) units, then the fused
+ * Abbe kernel. */
+size_t euv_plan_intensity_workspace_bytes(const euv_plan* plan, int n_clips, int n_mask_slices);
+int euv_plan_intensity(const euv_plan* plan, const uint8_t* d_masks, int n_clips,
+                       int n_mask_slices, double* d_image, void* d_work, size_t work_bytes,
+                       void* stream);
+/* ampS at one incidence for the NA-circle source orders (header.h:1394-1465):
+ * d_ax [clip][na source][n_orders]. */
+size_t euv_plan_amp_workspace_bytes(const euv_plan* plan, int n_clips, int n_mask_slices);
+int euv_plan_amp(const euv_plan* plan, int polar, double kx0, double ky0, const uint8_t* d_masks,
+                 int n_clips, int n_mask_slices, euv_c64* d_ax, void* d_work, size_t work_bytes,
+                 void* stream);
+/* M3D parameters of m3d.cpp:197-558 for polarisation pols[0]: d_a0, d_ax,
+ * d_ay [clip][ncut] (ax, ay zero where xinput == 0). */
+size_t euv_plan_m3d_workspace_bytes(const euv_plan* plan, int n_clips, int n_mask_slices);
+int euv_plan_m3d(euv_plan* plan, const uint8_t* d_masks, int n_clips, int n_mask_slices,
+                 euv_c64* d_a0, euv_c64* d_ax, euv_c64* d_ay, void* d_work, size_t work_bytes,
+                 void* stream);
+
+/* ------------------------------------------------------------------------ */
 /* Building blocks, exported for tests and for callers composing their own
  * pipelines. */
 
@@ -377,10 +502,12 @@ int euv_zgemm(int m, int n, int k, euv_c64 alpha, const double* d_scale, const e
 
 /* The bulk product of EUV_PREC_MIXED: same contract as euv_zgemm, computed on
  * the tcgen05 tensor cores as TF32x3 (each FP64 operand split into two TF32
- * terms, three TF32 products per real product, FP32 accumulation; ~1e-6
- * relative error per product).  Needs a workspace for the split operands.
- * d_status (optional device int): EUV_STATUS_TIMEOUT is OR-ed in if one of the
- * kernel's bounded waits (about 2 s) gave up. */
+ * terms inside the kernel, three TF32 products per real product, FP32
+ * accumulation; ~1e-6 relative error per product).  C must not overlap A or B
+ * (EUV_ERR_BAD_ARG).  d_status (optional device int): EUV_STATUS_TIMEOUT is
+ * OR-ed in if one of the kernel's bounded waits (about 2 s) gave up; without
+ * it the call keeps a per-call status word in d_work (256 bytes,
+ * euv_zgemm_tf32x3_workspace_bytes). */
 size_t euv_zgemm_tf32x3_workspace_bytes(int m, int n, int k, int batch);
 int euv_zgemm_tf32x3(int m, int n, int k, euv_c64 alpha, const double* d_scale,
                      const euv_c64* d_a, int lda, long long stride_a, const euv_c64* d_b, int ldb,
