@@ -46,6 +46,8 @@ def _args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-library-path", action="store_true",
                     help="skip timing the reference's cuSOLVER/cuBLAS/cuFFT sequence")
+    ap.add_argument("--no-served", action="store_true",
+                    help="skip the served-form leg (Poisson stream, mixed vs plain FP64)")
     return ap.parse_args()
 
 
@@ -328,6 +330,37 @@ def library_path_sample(plan, masks_dev, dev, units_per_clip: int, n_src_images:
                     % (n_src_images, cfg.xdiv)}
 
 
+SERVED_REQUESTS = 120
+SERVED_RATE = 50.0
+
+
+def served_leg(dev, n_requests: int = SERVED_REQUESTS, rate: float = SERVED_RATE):
+    """The served form (continuous batching) on a Poisson stream of seeded
+    clips: periods 256-2048 nm, order boxes 11x11-41x41, 50-200 source points,
+    X+Y; the mixed server (grouped launches) and the plain FP64 server (one
+    request per launch, one unit per call) on the same trace.  Latency per
+    request from arrival to its image in host memory."""
+    import torch
+    from euvlitho_b200 import serving as S
+    out = {"requests": n_requests, "rate_per_s": rate,
+           "workload": "Poisson arrivals of seeded clips, periods {256,512,1024,2048} nm, order "
+                       "boxes 11^2..41^2 (those valid for the period), 50-200 source points, X+Y"}
+    for name, kw in (("mixed", dict(precision="mixed")), ("plain_fp64", dict(plain=True))):
+        reqs = S.workload(n_requests, rate, seed=7)
+        srv = S.Server(device=dev, **kw)
+        t = time.perf_counter()
+        srv.warm(sorted({r.key for r in reqs}, key=lambda k: (k.period, k.box, k.n_src)))
+        st = srv.serve(reqs)
+        st["warm_s"] = time.perf_counter() - t - st["wall_s"]
+        out[name] = {k: st[k] for k in ("clips_per_s", "p50_ms", "p99_ms", "mean_batch",
+                                        "batches", "failed", "warm_s")}
+        del srv
+        torch.cuda.empty_cache()
+    out["clips_per_s_ratio"] = out["mixed"]["clips_per_s"] / out["plain_fp64"]["clips_per_s"]
+    out["p99_ratio"] = out["plain_fp64"]["p99_ms"] / out["mixed"]["p99_ms"]
+    return out
+
+
 # ---------------------------------------------------------------- clocks
 class Clocks:
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -381,6 +414,7 @@ def main() -> int:
     import torch.distributed as dist
     import numpy as np
     from euvlitho_b200 import _lib as L
+    from euvlitho_b200 import autotune
     from euvlitho_b200 import masks as MK
     from euvlitho_b200.config import preset
     from euvlitho_b200.engine import Plan
@@ -406,6 +440,14 @@ def main() -> int:
     host = MK.batch(cfg.ndivx, cfg.ndivy, rank_seeds(rank, CLIPS))
     b = plan.intensity_batch(CLIPS)
     b.masks.copy_(torch.from_numpy(host))
+    # the autotuner's picks for this step's shapes: cached per GPU model, else
+    # tuned now (first use), before the step is captured
+    t_tune = time.perf_counter()
+    tune = autotune.ensure(b)
+    tuning = {"tuned_now": tune["tuned"], "seconds": time.perf_counter() - t_tune,
+              "picks": {"%s/%d/%d" % k: v for k, v in tune["picks"].items()}}
+    if tune["tuned"]:
+        tuning.update(base_ms=tune["base_ms"], tuned_ms=tune["tuned_ms"])
     lib = L.lib()
     n0 = lib.euv_kernel_launches()
     b.run()
@@ -533,6 +575,13 @@ def main() -> int:
         except Exception as e:  # the baseline is reported, never required
             libpath = {"error": repr(e)}
 
+    served = None
+    if world == 1 and not a.no_served:
+        try:
+            served = served_leg(dev)
+        except Exception as e:  # reported, never required
+            served = {"error": repr(e)}
+
     out = {
         "metric": METRIC, "value": value, "unit": "clips/s", "n_gpus": world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
@@ -556,6 +605,8 @@ def main() -> int:
         "intensity_err_vs_oracle": err_oracle,
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
         "library_path_fp64": libpath,
+        "served": served,
+        "autotune": tuning,
         "gpu_launches": int(launches_per_step * a.steps),
         "clocks": clk,
     }

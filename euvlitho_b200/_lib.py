@@ -32,7 +32,7 @@ EUV_NOALLOC_SCRATCH_BYTES = 16 * 1024 * 1024
 EXPORTS = (
     "euv_version", "euv_last_error", "euv_kernel_launches",
     "euv_mask_spectrum_workspace_bytes", "euv_mask_spectrum",
-    "euv_amp_workspace_bytes", "euv_amp",
+    "euv_amp_workspace_bytes", "euv_amp", "euv_amp_euler_factors",
     "euv_abbe", "euv_m3d_fit",
     "euv_zgemm", "euv_zgemm_tf32x3_workspace_bytes", "euv_zgemm_tf32x3", "euv_lu_workspace_bytes", "euv_lu_factor", "euv_lu_solve",
     "euv_matfun_workspace_bytes", "euv_matfun_cs", "euv_matfun_cs_noalloc",
@@ -46,7 +46,11 @@ EXPORTS = (
     "euv_plan_upload", "euv_plan_check", "euv_plan_intensity_workspace_bytes",
     "euv_plan_intensity", "euv_plan_amp_workspace_bytes", "euv_plan_amp",
     "euv_plan_m3d_workspace_bytes", "euv_plan_m3d",
+    "euv_tune_set", "euv_tune_get", "euv_tune_clear",
 )
+EUV_KNOB_ABBE_SPLIT = 1
+EUV_KNOB_LU_CLUSTER = 2
+EUV_KNOB_ZGEMM_ROWS = 3
 EUV_ORDERS_DIAMOND = 0
 EUV_ORDERS_ELLIPSE = 1
 EUV_ORDERS_BOX = 2
@@ -95,7 +99,7 @@ class AmpDesc(C.Structure):
         ("d_kx0", P), ("d_ky0", P), ("d_polar", P), ("d_spec", P),
         ("n_src", C.c_int), ("d_src_order", P), ("d_src_2kz", P),
         ("precision", C.c_int), ("m_max", C.c_int), ("k0_max", C.c_double),
-        ("d_status", P),
+        ("d_status", P), ("d_dx", P), ("d_dy", P), ("euler_f", C.c_int),
     ]
 
 
@@ -201,6 +205,8 @@ def _declare(lib: C.CDLL) -> None:
     lib.euv_mask_spectrum.argtypes = [P, i, i, i, i, i, i, i, i, i, P, P, sz, P]
     lib.euv_amp_workspace_bytes.restype = sz
     lib.euv_amp_workspace_bytes.argtypes = [C.POINTER(AmpDesc)]
+    lib.euv_amp_euler_factors.restype = i
+    lib.euv_amp_euler_factors.argtypes = [C.POINTER(AmpDesc)]
     lib.euv_amp.restype = i
     lib.euv_amp.argtypes = [C.POINTER(AmpDesc), P, P, P, sz, P]
     lib.euv_abbe.restype = i
@@ -252,6 +258,12 @@ def _declare(lib: C.CDLL) -> None:
     lib.euv_cnn_predict.argtypes = [C.POINTER(CnnDesc), P, P, P, P, sz, P]
     lib.euv_cnn_downsample.restype = i
     lib.euv_cnn_downsample.argtypes = [i, P, P, P]
+    lib.euv_tune_set.restype = i
+    lib.euv_tune_set.argtypes = [i, i, i, i]
+    lib.euv_tune_get.restype = i
+    lib.euv_tune_get.argtypes = [i, i, i]
+    lib.euv_tune_clear.restype = None
+    lib.euv_tune_clear.argtypes = []
     PP = C.POINTER(P)
     lib.euv_config_reference.restype = None
     lib.euv_config_reference.argtypes = [C.POINTER(Config)]

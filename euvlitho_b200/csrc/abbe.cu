@@ -392,6 +392,8 @@ extern "C" int euv_abbe(const euv_abbe_desc* d, const euv_c64* d_ax, double* d_i
       nsplit = ns;
     }
   }
+  const int tuned = tune_lookup(EUV_KNOB_ABBE_SPLIT, d->n_units, d->n_src);
+  if (tuned > 0) nsplit = tuned < d->n_src ? tuned : d->n_src;
   p.nsplit = nsplit;
   dim3 grid(ystripes, nsplit, d->n_units);
   kerns[kv]<<<grid, AB_THREADS, smem, stream>>>(p, reinterpret_cast<const double2*>(d_ax), d_image);

@@ -1,6 +1,9 @@
 // Error reporting and version of the C ABI.
 #include <stdarg.h>
 #include <stdio.h>
+
+#include <mutex>
+
 #include "common.cuh"
 
 static thread_local char g_err[1024] = "";
@@ -44,4 +47,66 @@ extern "C" int euv_wait_probe(const int* d_flag, long long limit_ns, int* d_stat
                                                               d_status);
   EUV_LAUNCH_CHECK();
   return EUV_OK;
+}
+
+// ---------------------------------------------------------------- tuning table
+// Picks written by an autotuner (or by hand) that override a kernel's built-in
+// choice for one problem shape; looked up on the host at every launch.
+namespace {
+struct TuneEntry {
+  int knob, k0, k1, value;
+};
+constexpr int kTuneCap = 1024;
+TuneEntry g_tune[kTuneCap];
+int g_tune_n = 0;
+std::mutex g_tune_mu;
+
+bool knob_value_ok(int knob, int value) {
+  switch (knob) {
+    case EUV_KNOB_ABBE_SPLIT: return value >= 1 && value <= 64;
+    case EUV_KNOB_LU_CLUSTER: return value == 1 || value == 2 || value == 4 || value == 8;
+    case EUV_KNOB_ZGEMM_ROWS: return value == 32 || value == 64;
+    default: return false;
+  }
+}
+}  // namespace
+
+namespace euv {
+int tune_lookup(int knob, int k0, int k1) {
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  for (int i = 0; i < g_tune_n; ++i)
+    if (g_tune[i].knob == knob && g_tune[i].k0 == k0 && g_tune[i].k1 == k1) return g_tune[i].value;
+  return 0;
+}
+}  // namespace euv
+
+extern "C" int euv_tune_set(int knob, int k0, int k1, int value) {
+  if (value != 0 && !knob_value_ok(knob, value)) {
+    euv_set_error("euv_tune_set: value %d not allowed for knob %d", value, knob);
+    return EUV_ERR_BAD_ARG;
+  }
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  for (int i = 0; i < g_tune_n; ++i)
+    if (g_tune[i].knob == knob && g_tune[i].k0 == k0 && g_tune[i].k1 == k1) {
+      if (value == 0) {
+        g_tune[i] = g_tune[--g_tune_n];
+      } else {
+        g_tune[i].value = value;
+      }
+      return EUV_OK;
+    }
+  if (value == 0) return EUV_OK;
+  if (g_tune_n >= kTuneCap) {
+    euv_set_error("euv_tune_set: table full (%d entries)", kTuneCap);
+    return EUV_ERR_BAD_ARG;
+  }
+  g_tune[g_tune_n++] = TuneEntry{knob, k0, k1, value};
+  return EUV_OK;
+}
+
+extern "C" int euv_tune_get(int knob, int k0, int k1) { return euv::tune_lookup(knob, k0, k1); }
+
+extern "C" void euv_tune_clear(void) {
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  g_tune_n = 0;
 }

@@ -108,6 +108,9 @@ extern "C" void euv_set_error(const char* fmt, ...);
 extern "C" void euv_count_launch(void);
 
 namespace euv {
+// The tuning table's pick for (knob, k0, k1), 0 when there is none (api.cu).
+int tune_lookup(int knob, int k0, int k1);
+
 // Raise a kernel's dynamic shared-memory limit once per device (the first call
 // happens outside any stream capture; later calls do nothing).
 template <typename K>

@@ -448,11 +448,13 @@ static int panel_sub(int n, int j0) { return n - j0 <= 8 * LC_THREADS ? 1 : 0; }
 static int lu_panel(int n, int j0, int jb, double2* A, long long lda, long long sa, int* ipiv,
                     int* info, int batch, cudaStream_t st) {
   const int rows = n - j0;
-  if (rows <= LC_THREADS)
+  // the tuning table may spread a panel's rows over more CTAs than they need
+  const int lc_min = tune_lookup(EUV_KNOB_LU_CLUSTER, n, batch);
+  if (rows <= LC_THREADS && lc_min <= 1)
     lu_panel_cluster_kernel<1><<<batch, LC_THREADS, 0, st>>>(n, j0, jb, A, lda, sa, ipiv, info);
-  else if (rows <= 2 * LC_THREADS)
+  else if (rows <= 2 * LC_THREADS && lc_min <= 2)
     lu_panel_cluster_kernel<2><<<2 * batch, LC_THREADS, 0, st>>>(n, j0, jb, A, lda, sa, ipiv, info);
-  else if (rows <= 4 * LC_THREADS)
+  else if (rows <= 4 * LC_THREADS && lc_min <= 4)
     lu_panel_cluster_kernel<4><<<4 * batch, LC_THREADS, 0, st>>>(n, j0, jb, A, lda, sa, ipiv, info);
   else if (rows <= 8 * LC_THREADS)
     lu_panel_cluster_kernel<8><<<8 * batch, LC_THREADS, 0, st>>>(n, j0, jb, A, lda, sa, ipiv, info);

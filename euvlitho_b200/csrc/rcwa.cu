@@ -38,7 +38,7 @@ int gemm_mixed(int m, int n, int k, cplx alpha, const double* scale, const doubl
                long long lda, long long sa, const double2* b, long long ldb, long long sb,
                cplx beta, double2* c, long long ldc, long long sc, cplx diag, int batch,
                const int* steps, int step, void* work, size_t work_bytes, int* status,
-               cudaStream_t stream, int reuse, const double2* cin);
+               cudaStream_t stream, const double2* cin);
 size_t gemm_mixed_workspace_bytes(int m, int n, int k, int batch);
 
 // ||A||_1 bound for the degree-8 Taylor step of cos/sin(sqrt(A)): the dropped
@@ -196,6 +196,8 @@ __global__ void twiddle_kernel(int rows, int cols, int roff, int coff, int fdiv,
 // ---------------------------------------------------------------- D and G
 struct SliceParams {
   double k, dx, dy;
+  const double* dxs;  // per-unit periods (NULL: dx, dy for every unit)
+  const double* dys;
   int n, lmax, mmax, lr2, mr2, n_slices, slice;
   cplx eps_m1;   // eps_abs - 1
   cplx sig_m1;   // 1/eps_abs - 1
@@ -221,8 +223,9 @@ __global__ void build_dg_kernel(SliceParams p, const double2* spectra, const int
   const cplx F = mk(f2.x, f2.y);
   const bool dc = (l == 2 * p.lmax) && (m == 2 * p.mmax);
   const double twopi = 6.283185307179586476925286766559;
-  const double kxi = kx0[u] + twopi * li / p.dx, kyi = ky0[u] + twopi * mi / p.dy;
-  const double kxj = kx0[u] + twopi * lj / p.dx, kyj = ky0[u] + twopi * mj / p.dy;
+  const double dxu = p.dxs ? p.dxs[u] : p.dx, dyu = p.dys ? p.dys[u] : p.dy;
+  const double kxi = kx0[u] + twopi * li / dxu, kyi = ky0[u] + twopi * mi / dyu;
+  const double kxj = kx0[u] + twopi * lj / dxu, kyj = ky0[u] + twopi * mj / dyu;
   const int pol = polar[u];
   if (want_d) {
     cplx eps = p.eps_m1 * F;
@@ -231,9 +234,9 @@ __global__ void build_dg_kernel(SliceParams p, const double2* spectra, const int
     cplx v = (p.k * p.k) * eps;
     if (pol == 0) {
       // -i * eta * kx_j, eta = i 2 pi l / dx * leps  ->  +2 pi l/dx * leps * kx_j
-      v = v + (twopi * (double)(l - 2 * p.lmax) / p.dx * kxj) * leps;
+      v = v + (twopi * (double)(l - 2 * p.lmax) / dxu * kxj) * leps;
     } else {
-      v = v + (twopi * (double)(m - 2 * p.mmax) / p.dy * kyj) * leps;
+      v = v + (twopi * (double)(m - 2 * p.mmax) / dyu * kyj) * leps;
     }
     if (i == j) v.x -= kxi * kxi + kyi * kyi;
     D[(long long)u * nn + t] = make_double2(v.x, v.y);
@@ -281,6 +284,8 @@ struct StackParams {
   double dmo, dmosi, dsi, dsimo, dsiru, dru;
   int nml;
   double dx, dy;
+  const double* dxs;  // per-unit periods (NULL: dx, dy for every unit)
+  const double* dys;
   int n;
 };
 
@@ -318,8 +323,8 @@ __global__ void multilayer_kernel(StackParams p, const int* lidx, const int* mid
   if (t >= p.n * n_units) return;
   const int u = t / p.n, i = t % p.n;
   const double twopi = 6.283185307179586476925286766559;
-  const double kx = kx0[u] + twopi * lidx[i] / p.dx;
-  const double ky = ky0[u] + twopi * midx[i] / p.dy;
+  const double kx = kx0[u] + twopi * lidx[i] / (p.dxs ? p.dxs[u] : p.dx);
+  const double ky = ky0[u] + twopi * midx[i] / (p.dys ? p.dys[u] : p.dy);
   const double kxy2 = kx * kx + ky * ky;
   const double k = p.k, k2 = k * k;
   const double kp = polar[u] == 0 ? kx : ky;
@@ -547,12 +552,6 @@ __global__ void flag_singular_kernel(const int* info, int n, int* status) {
 
 // GEMM dispatch by precision (FP64 DMMA, or TF32x3 tcgen05 tensor cores for
 // the bulk products of the mixed form; `status` receives EUV_STATUS_TIMEOUT).
-// Gemm reuse flags (mixed form only): the previous call through the same Gemm
-// split this unchanged operand in the same role and shape, so its TF32 planes
-// in the workspace are current.
-constexpr int kReuseA = 1;
-constexpr int kReuseB = 2;
-
 struct Gemm {
   int precision;
   void* mwork;
@@ -562,11 +561,11 @@ struct Gemm {
   int operator()(int m, int n, int k, cplx alpha, const double* scale, const double2* a,
                  long long lda, long long sa, const double2* b, long long ldb, long long sb,
                  cplx beta, double2* c, long long ldc, long long sc, cplx diag, int batch,
-                 const int* steps = nullptr, int step = 0, int reuse = 0,
+                 const int* steps = nullptr, int step = 0,
                  const double2* cin = nullptr) const {
     if (precision == EUV_PREC_MIXED)
       return gemm_mixed(m, n, k, alpha, scale, a, lda, sa, b, ldb, sb, beta, c, ldc, sc, diag,
-                        batch, steps, step, mwork, mbytes, status, stream, reuse, cin);
+                        batch, steps, step, mwork, mbytes, status, stream, cin);
     if (cin != nullptr && cin != c) {
       // FP64 GEMM: the beta term reads C, so C = Cin first (same shape)
       const size_t span = (size_t)(batch - 1) * sc + (size_t)(n - 1) * ldc + m;
@@ -604,18 +603,17 @@ int matfun(int n, int batch, const double2* D, const double* thick, double2** pc
   int rc;
   // P2 = h^4 D D, P3 = h^2 P2 D, P4 = P2 P2
   if ((rc = gemm(n, n, n, one, w.h4, D, n, nn, D, n, nn, zero, w.P2, n, nn, zero, batch))) return rc;
-  if ((rc = gemm(n, n, n, one, w.h2, w.P2, n, nn, D, n, nn, zero, w.P3, n, nn, zero, batch, nullptr, 0,
-                 kReuseB))) return rc;  // D as B again
-  if ((rc = gemm(n, n, n, one, nullptr, w.P2, n, nn, w.P2, n, nn, zero, w.P4, n, nn, zero, batch,
-                 nullptr, 0, kReuseA))) return rc;  // P2 as A again
+  if ((rc = gemm(n, n, n, one, w.h2, w.P2, n, nn, D, n, nn, zero, w.P3, n, nn, zero, batch))) return rc;
+  if ((rc = gemm(n, n, n, one, nullptr, w.P2, n, nn, w.P2, n, nn, zero, w.P4, n, nn, zero, batch)))
+    return rc;
   double2* C = *pc;
   double2* S = *ps;
   taylor_prep_kernel<<<ge, bs, 0, stream>>>(n, batch, D, w.P2, w.P3, w.P4, w.h, w.h2, C, w.T1, S,
                                             w.T2);
   EUV_LAUNCH_CHECK();
   if ((rc = gemm(n, n, n, one, nullptr, w.P4, n, nn, w.T1, n, nn, one, C, n, nn, zero, batch))) return rc;
-  if ((rc = gemm(n, n, n, one, nullptr, w.P4, n, nn, w.T2, n, nn, one, S, n, nn, zero, batch,
-                 nullptr, 0, kReuseA))) return rc;  // P4 as A again
+  if ((rc = gemm(n, n, n, one, nullptr, w.P4, n, nn, w.T2, n, nn, one, S, n, nn, zero, batch)))
+    return rc;
   // double-angle steps; entries with fewer steps copy through (C = A)
   double2* tS = w.P2;
   double2* tC = w.P3;
@@ -624,7 +622,7 @@ int matfun(int n, int batch, const double2* D, const double* thick, double2** pc
                    batch, w.steps, step)))
       return rc;
     if ((rc = gemm(n, n, n, mk(2.0, 0.0), nullptr, C, n, nn, C, n, nn, zero, tC, n, nn,
-                   mk(-1.0, 0.0), batch, w.steps, step, kReuseB)))  // C as B again
+                   mk(-1.0, 0.0), batch, w.steps, step)))
       return rc;
     double2* t = S;
     S = tS;
@@ -757,7 +755,8 @@ static int check_desc(const euv_amp_desc* d) {
       d->n_slices > EUV_MAX_SLICES || d->n_src < 0 || d->k <= 0 || d->dx <= 0 || d->dy <= 0 ||
       !d->d_lindex || !d->d_mindex || !d->d_kx0 || !d->d_ky0 || !d->d_polar || !d->d_spec ||
       (d->n_src > 0 && (!d->d_src_order || !d->d_src_2kz)) ||
-      (d->precision != EUV_PREC_FP64 && d->precision != EUV_PREC_MIXED))
+      (d->precision != EUV_PREC_FP64 && d->precision != EUV_PREC_MIXED) || d->euler_f < -1 ||
+      d->euler_f > 8)
     return 0;
   for (int n = 0; n < d->n_slices; ++n)
     if (!(d->dabs[n] >= 0.0) || (d->eabs[n].re == 0.0 && d->eabs[n].im == 0.0)) return 0;
@@ -767,6 +766,17 @@ static int check_desc(const euv_amp_desc* d) {
 }  // namespace euv
 
 using namespace euv;
+
+extern "C" int euv_amp_euler_factors(const euv_amp_desc* d) {
+  if (!d || !check_desc(d)) {
+    euv_set_error("euv_amp_euler_factors: invalid descriptor");
+    return -2;
+  }
+  if (d->precision != EUV_PREC_MIXED) return 0;
+  if (d->euler_f != 0) return d->euler_f;
+  const int f = euler_factors(d);
+  return f > 0 ? f : -1;
+}
 
 extern "C" size_t euv_amp_workspace_bytes(const euv_amp_desc* d) {
   if (!check_desc(d)) return 0;
@@ -818,6 +828,8 @@ extern "C" int euv_amp(const euv_amp_desc* d, const euv_c64* d_spectra, euv_c64*
   sp.k = d->k;
   sp.dx = d->dx;
   sp.dy = d->dy;
+  sp.dxs = d->d_dx;
+  sp.dys = d->d_dy;
   sp.n = N;
   sp.lmax = d->lmax;
   sp.mmax = d->mmax;
@@ -851,6 +863,8 @@ extern "C" int euv_amp(const euv_amp_desc* d, const euv_c64* d_spectra, euv_c64*
   stp.nml = d->stack.nml;
   stp.dx = d->dx;
   stp.dy = d->dy;
+  stp.dxs = d->d_dx;
+  stp.dys = d->d_dy;
   stp.n = N;
   multilayer_kernel<<<grid1((long long)N * U, 128), 128, 0, stream>>>(
       stp, d->d_lindex, d->d_mindex, d->d_kx0, d->d_ky0, d->d_polar, w.x2, w.y2, w.gx2, w.klm, U);
@@ -860,27 +874,25 @@ extern "C" int euv_amp(const euv_amp_desc* d, const euv_c64* d_spectra, euv_c64*
   MatfunBufs mb{w.P2, w.P3, w.P4, w.T1, w.W, w.norm, w.h, w.h2, w.h4, w.steps, status};
   // Mixed form: G^-1 by the Euler product (I - E)^-1 = prod_f (I + E^(2^f)),
   // f < euler_f, when the config bound on ||E||_2 makes it converge fast.
-  const int euler_f = d->precision == EUV_PREC_MIXED ? euler_factors(d) : 0;
+  const int euler_f = d->precision != EUV_PREC_MIXED ? 0
+                      : d->euler_f > 0                ? d->euler_f
+                      : d->euler_f < 0                ? 0
+                                                      : euler_factors(d);
   // factors f = 1..euler_f-1 applied to the partial product held in Zbuf (the
   // f = 0 factor is applied by the caller); E^(2^f) ping-pongs between G and P2
-  // g_split: the caller's last GEMM had G as its A operand
-  auto euler_tail = [&](double2* Zbuf, bool g_split) -> int {
+  auto euler_tail = [&](double2* Zbuf) -> int {
     double2* P = w.G;
     double2* Pn = w.P2;
     double2* Zc = Zbuf;
     double2* Zt = w.W;
     for (int f = 1; f < euler_f; ++f) {
-      // P as A again: split by the previous factor's P Zc (or the caller's G Z)
-      const int ru = (f > 1 || g_split) ? kReuseA : 0;
-      int r2 = gemm(N, N, N, one, nullptr, P, N, nn, P, N, nn, zero, Pn, N, nn, zero, U, nullptr, 0,
-                    ru);
+      int r2 = gemm(N, N, N, one, nullptr, P, N, nn, P, N, nn, zero, Pn, N, nn, zero, U);
       if (r2) return r2;
       double2* t = P;
       P = Pn;
       Pn = t;
       // Zt = P Zc + Zc (the beta term read from Zc)
-      r2 = gemm(N, N, N, one, nullptr, P, N, nn, Zc, N, nn, one, Zt, N, nn, zero, U, nullptr, 0, 0,
-                Zc);
+      r2 = gemm(N, N, N, one, nullptr, P, N, nn, Zc, N, nn, one, Zt, N, nn, zero, U, nullptr, 0, Zc);
       if (r2) return r2;
       t = Zc;
       Zc = Zt;
@@ -907,7 +919,7 @@ extern "C" int euv_amp(const euv_amp_desc* d, const euv_c64* d_spectra, euv_c64*
       // product on the tensor cores (E was built in place of G)
       euler_first_diag_kernel<<<ge, bs, 0, stream>>>(N, cdiv(one, mk(0.0, d->k)), w.G, w.gx2, w.Z);
       EUV_LAUNCH_CHECK();
-      if ((rc = euler_tail(w.Z, false))) return rc;
+      if ((rc = euler_tail(w.Z))) return rc;
       Zp = w.Z;
     } else if (bottom) {
       // Z = G^-1 diag(Bru (URUU+URUB))
@@ -925,11 +937,11 @@ extern "C" int euv_amp(const euv_amp_desc* d, const euv_c64* d_spectra, euv_c64*
                                              d->d_kx0, d->d_ky0, d->d_polar, nullptr, w.Gp, 0, 2);
       EUV_LAUNCH_CHECK();
       if ((rc = gemm(N, N, N, mk(-1.0, 0.0), nullptr, w.Gp, N, nn, X, N, nn, one, w.Z, N, nn, zero,
-                     U, nullptr, 0, 0, X))) return rc;  // Z = X - Gp X
+                     U, nullptr, 0, X))) return rc;  // Z = X - Gp X
       if ((rc = gemm(N, N, N, one, nullptr, w.G, N, nn, w.Z, N, nn, one, w.W, N, nn, zero, U,
-                     nullptr, 0, 0, w.Z))) return rc;  // W = Z + G Z
+                     nullptr, 0, w.Z))) return rc;  // W = Z + G Z
       EUV_CUDA_TRY(cudaMemcpyAsync(w.Z, w.W, (size_t)U * nn * sizeof(double2), cudaMemcpyDeviceToDevice, stream));
-      if ((rc = euler_tail(w.Z, true))) return rc;
+      if ((rc = euler_tail(w.Z))) return rc;
       Zp = w.Z;
     } else if (d->refresh_sigma) {
       // Z = G_n^-1 G_{n+1} X
@@ -956,11 +968,9 @@ extern "C" int euv_amp(const euv_amp_desc* d, const euv_c64* d_spectra, euv_c64*
     double2* Wb = fr[0];
     double2* Xn = fr[1];
     double2* Yn = fr[2];
-    // W = S Z ; Xn = C Z - i S Y ; Yn = -i D W + C Y, ordered so that three of
-    // the five products find one operand already split
+    // W = S Z ; Xn = C Z - i S Y ; Yn = -i D W + C Y
     if ((rc = gemm(N, N, N, one, nullptr, S, N, nn, Zp, N, nn, zero, Wb, N, nn, zero, U))) return rc;
-    if ((rc = gemm(N, N, N, one, nullptr, C, N, nn, Zp, N, nn, zero, Xn, N, nn, zero, U, nullptr, 0,
-                   kReuseB))) return rc;  // Zp as B again
+    if ((rc = gemm(N, N, N, one, nullptr, C, N, nn, Zp, N, nn, zero, Xn, N, nn, zero, U))) return rc;
     if (bottom) {
       if ((rc = gemm(N, N, N, mi, nullptr, w.D, N, nn, Wb, N, nn, zero, Yn, N, nn, zero, U))) return rc;
       colscale_kernel<<<ge, bs, 0, stream>>>(N, mi, S, w.y2, one, Xn);
@@ -968,10 +978,8 @@ extern "C" int euv_amp(const euv_amp_desc* d, const euv_c64* d_spectra, euv_c64*
       colscale_kernel<<<ge, bs, 0, stream>>>(N, one, C, w.y2, one, Yn);
       EUV_LAUNCH_CHECK();
     } else {
-      if ((rc = gemm(N, N, N, one, nullptr, C, N, nn, Y, N, nn, zero, Yn, N, nn, zero, U, nullptr,
-                     0, kReuseA))) return rc;  // C as A again
-      if ((rc = gemm(N, N, N, mi, nullptr, S, N, nn, Y, N, nn, one, Xn, N, nn, zero, U, nullptr, 0,
-                     kReuseB))) return rc;  // Y as B again
+      if ((rc = gemm(N, N, N, one, nullptr, C, N, nn, Y, N, nn, zero, Yn, N, nn, zero, U))) return rc;
+      if ((rc = gemm(N, N, N, mi, nullptr, S, N, nn, Y, N, nn, one, Xn, N, nn, zero, U))) return rc;
       if ((rc = gemm(N, N, N, mi, nullptr, w.D, N, nn, Wb, N, nn, one, Yn, N, nn, zero, U))) return rc;
     }
     if (n == 0) {

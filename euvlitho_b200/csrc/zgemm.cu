@@ -267,6 +267,13 @@ int zgemm_launch(const GemmArgs& p, int batch, cudaStream_t stream, bool upd = f
     dim3 grid((p.m + GBM - 1) / GBM, (p.n + GBN - 1) / GBN, batch);
     EUV_CUDA_TRY(ensure_smem(zgemm_kernel<true, 4, GSTAGES>, (int)sm, smem_done_upd));
     zgemm_kernel<true, 4, GSTAGES><<<grid, GTHREADS, sm, stream>>>(p);
+  } else if (tune_lookup(EUV_KNOB_ZGEMM_ROWS, p.m, batch) == 32) {
+    // 32 x 64 tiles: twice the CTAs, for shapes that leave SMs idle with 64 rows
+    static int smem_done32[64];
+    constexpr size_t sm = zgemm_smem<2, GSTAGES>();
+    dim3 grid((p.m + 31) / 32, (p.n + GBN - 1) / GBN, batch);
+    EUV_CUDA_TRY(ensure_smem(zgemm_kernel<false, 2, GSTAGES>, (int)sm, smem_done32));
+    zgemm_kernel<false, 2, GSTAGES><<<grid, GTHREADS, sm, stream>>>(p);
   } else {
     dim3 grid((p.m + GBM - 1) / GBM, (p.n + GBN - 1) / GBN, batch);
     EUV_CUDA_TRY(ensure_smem(zgemm_kernel<false, 4, GSTAGES>, (int)GSMEM, smem_done));

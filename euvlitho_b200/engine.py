@@ -244,11 +244,20 @@ class Plan:
         return ax, srcs
 
     # ------------------------------------------------------------ Abbe
-    def abbe_tables(self):
-        if self._abbe_tables is not None:
-            return self._abbe_tables
+    def abbe_tables(self, n_src: Optional[int] = None):
+        """Resident Abbe tables of every (polarisation, family), with ``n_src``
+        source slots per table (default: the largest family; more pads with
+        empty slots, so that batches of different configurations share one
+        source stride)."""
+        need = max(len(f.pts) for f in self.fams)
+        n_src = need if n_src is None else int(n_src)
+        if n_src < need:
+            raise ValueError("n_src %d is below the largest family (%d)" % (n_src, need))
+        if self._abbe_tables is None:
+            self._abbe_tables = {}
+        if n_src in self._abbe_tables:
+            return self._abbe_tables[n_src]
         cfg = self.cfg
-        n_src = max(len(f.pts) for f in self.fams)
         coefs, nidxs, kx0s, ky0s, orders, kz2s, pols, nsrcs = [], [], [], [], [], [], [], []
         for p in self.pols:
             for f in self.fams:
@@ -275,7 +284,7 @@ class Plan:
             kx0=np.array(kx0s), ky0=np.array(ky0s), order=np.stack(orders), kz2=np.stack(kz2s),
             pol=np.array(pols, np.int32), nsrc=np.array(nsrcs, np.int32),
         )
-        self._abbe_tables = tb
+        self._abbe_tables[n_src] = tb
         return tb
 
     def intensity_batch(self, n_clips: int, n_mask_slices: int = 1) -> "IntensityBatch":

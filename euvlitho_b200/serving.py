@@ -3,21 +3,28 @@
 Requests are single clips with their own optical configuration (period, order
 box, source points, polarisations).  The server keeps, per configuration, a
 resident :class:`~euvlitho_b200.engine.Plan` (order/pupil/source tables and the
-Abbe E-field factors) and prepared batches (per-unit tables, spectra, amplitude
-and image buffers) for 1, 2, 4, .. max_batch clips.  One host loop:
+Abbe E-field factors).  One host loop:
 
-* admits the requests that have arrived into per-configuration queues;
-* whenever one of ``n_streams`` stream slots is idle, launches the oldest
-  waiting configuration with up to ``max_batch`` of its requests -- requests
-  that arrived while other batches were running join the next launch
-  (continuous batching), and batches of different configurations run on
-  different streams at the same time (their kernels overlap on the device);
-* admits a batch only when its workspace fits in the free part of the HBM
-  arena (``hbm_budget`` bytes, first fit), so the batches in flight never
-  exceed the budget; large configurations run their units in chunks so one
-  launch needs at most half of the arena;
+* admits the requests that have arrived into per-group queues: a group is an
+  order box with its polarisations, so requests of different periods and
+  source counts share a queue (``GroupKey``);
+* whenever one of ``n_streams`` stream slots is idle, launches the group of
+  the oldest waiting request with up to ``max_batch`` of its requests: one
+  batched ampS of all their (clip, family, polarisation) units, each unit with
+  its own clip period, then one fused Abbe launch per configuration.  Requests
+  that arrived while other launches were running join the next launch
+  (continuous batching), and launches on different streams overlap on the
+  device;
+* admits a launch only when its device block fits in the free part of the
+  HBM arena (``hbm_budget`` bytes, first fit) and uses at most half of it, so
+  the launches in flight never exceed the budget;
 * polls CUDA events to complete requests and records their latency from
   arrival to the image being in host memory.
+
+A clip's result does not depend on the other clips of its launch: every
+group has one fixed Euler factor count (``Server.group_euler``) and the
+double-angle steps are per unit.  ``plain=True`` is the unbatched FP64 form
+(one request per launch, one unit per ampS call).
 
 The reference has no serving layer (its drivers read one ``mask.bin`` and write
 one file); this is the north-star serving form of the same computation.
@@ -25,6 +32,7 @@ one file); this is the north-star serving form of the same computation.
 from __future__ import annotations
 
 import collections
+import ctypes as C
 import dataclasses
 import math
 import time
@@ -161,19 +169,250 @@ class Executor:
         return ev
 
 
+# Source slots of every Abbe table in grouped launches (the largest source
+# count a request may ask for): one source stride for all configurations.
+MAX_SOURCES = 200
+
+
+@dataclasses.dataclass(frozen=True)
+class GroupKey:
+    """Requests that can share one ampS launch: the same order box (hence the
+    same order set and matrix size) and polarisations.  Their periods and
+    source counts may differ: each unit carries its own period (euv_amp_desc
+    d_dx / d_dy), source columns and Abbe tables."""
+
+    box: int
+    pols: Tuple[str, ...]
+
+
+def group_of(key: ClipKey) -> GroupKey:
+    return GroupKey(key.box, key.pols)
+
+
+def _al(n: int) -> int:
+    return (int(n) + 255) & ~255
+
+
+class Slot:
+    """One stream of the server with its device status word and pinned
+    staging buffers (grown on demand, reused once the slot's launch is done)."""
+
+    def __init__(self, device):
+        self.stream = torch.cuda.Stream(device=device)
+        self.status = torch.zeros(1, dtype=torch.int32, device=device)
+        self.hstat = torch.zeros(1, dtype=torch.int32).pin_memory()
+        self.hin = torch.zeros(0, dtype=torch.uint8)
+        self.hout = torch.zeros(0, dtype=torch.float64)
+
+    def staging(self, nin: int, nout: int) -> None:
+        if self.hin.numel() < nin:
+            self.hin = torch.zeros(nin, dtype=torch.uint8).pin_memory()
+        if self.hout.numel() < nout:
+            self.hout = torch.zeros(nout, dtype=torch.float64).pin_memory()
+
+
+class GroupLaunch:
+    """Host side of one launch of a group: the requests ordered by
+    configuration, the per-unit tables, the device layout and its size.
+
+    Units are clip-major within each configuration; configuration c holds
+    clips [c0, c0 + n) and units [u0, u0 + n * tables).  Device region (one
+    arena block): masks | per-unit tables | spectra | Ax | images | scratch;
+    masks and tables are staged in pinned memory with the same layout and go
+    over in one copy."""
+
+    def __init__(self, server: "Server", group: GroupKey, reqs: List[Request]):
+        self.group = group
+        self.reqs = sorted(reqs, key=lambda r: (r.key.period, r.key.n_src, r.arrival))
+        pad = server.n_src_pad
+        parts = []  # (plan, tables, [requests])
+        for r in self.reqs:
+            if parts and parts[-1][2][0].key == r.key:
+                parts[-1][2].append(r)
+            else:
+                plan = server.plan(r.key)
+                parts.append((plan, plan.abbe_tables(pad), [r]))
+        self.parts = parts
+        p0 = parts[0][0]
+        self.N = p0.orders.n
+        self.npol = len(group.pols)
+        self.nabs = p0.cfg.nabs
+        self.S = (4 * p0.orders.lmax + 1) * (4 * p0.orders.mmax + 1)
+        kx0, ky0, dx, dy, pol, spec, order, kz2 = [], [], [], [], [], [], [], []
+        tab, img, nsrc, invw = [], [], [], []
+        self.part_units, self.part_images, self.part_masks, self.part_clip0 = [], [], [], []
+        mask_off = img_off = 0
+        ci = 0
+        for plan, tb, rs in parts:
+            ntab = len(tb["pol"])
+            nf = len(plan.fams)
+            cfg = plan.cfg
+            u0 = len(kx0)
+            self.part_clip0.append(ci)
+            for j in range(len(rs)):
+                for t in range(ntab):
+                    kx0.append(tb["kx0"][t])
+                    ky0.append(tb["ky0"][t])
+                    dx.append(cfg.dx)
+                    dy.append(cfg.dy)
+                    pol.append(tb["pol"][t])
+                    spec.append(ci + j)
+                    order.append(tb["order"][t])
+                    kz2.append(tb["kz2"][t])
+                    tab.append(t)
+                    img.append(j * self.npol + t // nf)
+                    nsrc.append(tb["nsrc"][t])
+            invw += [1.0 / plan.sdivsum] * (len(rs) * self.npol)
+            self.part_units.append((u0, len(kx0) - u0))
+            nb = cfg.ndivx * cfg.ndivy // 8
+            self.part_masks.append((mask_off, nb))
+            mask_off += len(rs) * nb
+            isz = self.npol * cfg.xdiv * cfg.ydiv
+            self.part_images.append((img_off, isz))
+            img_off += len(rs) * isz
+            ci += len(rs)
+        self.n_clips = ci
+        self.U = U = len(kx0)
+        self.k0_max = float(max(np.abs(kx0).max(), np.abs(ky0).max()))
+        self.dx_min, self.dy_min = float(min(dx)), float(min(dy))
+        # host tables, in device layout order
+        arrays = [np.asarray(kx0, np.float64), np.asarray(ky0, np.float64),
+                  np.asarray(dx, np.float64), np.asarray(dy, np.float64),
+                  np.asarray(pol, np.int32), np.asarray(spec, np.int32),
+                  np.asarray(order, np.int32).reshape(-1), np.asarray(kz2, np.float64).reshape(-1),
+                  np.asarray(tab, np.int32), np.asarray(img, np.int32),
+                  np.asarray(nsrc, np.int32), np.asarray(invw, np.float64)]
+        self.table_offsets = []
+        off = _al(mask_off)
+        for a in arrays:
+            self.table_offsets.append(off)
+            off += _al(a.nbytes)
+        self.arrays = arrays
+        self.in_bytes = off                         # masks + tables: the staged part
+        self.spec_off = off
+        off += _al(self.n_clips * self.nabs * self.S * 16)
+        self.ax_off = off
+        off += _al(U * pad * self.N * 16)
+        self.img_off = off
+        self.img_count = img_off
+        off += _al(img_off * 8)
+        self.scratch_off = off
+        desc = self._desc(server, 0)
+        amp = L.lib().euv_amp_workspace_bytes(C.byref(desc))
+        if amp == 0:
+            raise ValueError("invalid ampS descriptor for group %s" % (group,))
+        spec_ws = max(L.lib().euv_mask_spectrum_workspace_bytes(
+            len(rs), plan.cfg.ndivx, plan.cfg.ndivy, plan.cfg.fdivx, plan.cfg.fdivy,
+            2 * plan.orders.lmax, 2 * plan.orders.mmax) for plan, _, rs in parts)
+        self.scratch_bytes = _al(max(amp, spec_ws))
+        self.need = off + self.scratch_bytes
+
+    def _desc(self, server: "Server", base: int) -> L.AmpDesc:
+        """ampS descriptor of the launch; ``base`` = device address of the block
+        (0 while sizing)."""
+        p0 = self.parts[0][0]
+        d = p0.amp_desc(p0.orders, p0._t_l, p0._t_m, torch.zeros(1, dtype=torch.float64),
+                        torch.zeros(1, dtype=torch.float64), torch.zeros(1, dtype=torch.int32),
+                        torch.zeros(1, dtype=torch.int32), torch.zeros((1, 1), dtype=torch.int32),
+                        torch.zeros((1, 1), dtype=torch.float64), [])
+        d.dx, d.dy = self.dx_min, self.dy_min
+        d.n_units = self.U
+        d.n_src = server.n_src_pad
+        d.k0_max = self.k0_max
+        d.euler_f = server.group_euler(self.group)
+        o = self.table_offsets
+        if base:
+            d.d_kx0, d.d_ky0, d.d_dx, d.d_dy = base + o[0], base + o[1], base + o[2], base + o[3]
+            d.d_polar, d.d_spec, d.d_src_order, d.d_src_2kz = (base + o[4], base + o[5],
+                                                               base + o[6], base + o[7])
+        return d
+
+    def launch(self, server: "Server", slot: Slot, work: torch.Tensor) -> torch.cuda.Event:
+        base = work.data_ptr()
+        slot.staging(self.in_bytes, self.img_count)
+        hin = slot.hin.numpy()
+        for (plan, _, rs), (moff, nb) in zip(self.parts, self.part_masks):
+            for j, r in enumerate(rs):
+                hin[moff + j * nb:moff + (j + 1) * nb] = r.mask
+        for off, a in zip(self.table_offsets, self.arrays):
+            hin[off:off + a.nbytes] = a.view(np.uint8)
+        st = slot.stream.cuda_stream
+        with torch.cuda.stream(slot.stream):
+            work[:self.in_bytes].copy_(slot.hin[:self.in_bytes], non_blocking=True)
+            scratch = base + self.scratch_off
+            for (plan, _, rs), (moff, nb), c0 in zip(self.parts, self.part_masks,
+                                                     self.part_clip0):
+                cfg = plan.cfg
+                out = base + self.spec_off + c0 * self.nabs * self.S * 16
+                if self.nabs > 1:
+                    raise ValueError("grouped serving takes one absorber slice")
+                L.call("euv_mask_spectrum", base + moff, len(rs), cfg.ndivx, cfg.ndivy, cfg.fdivx,
+                       cfg.fdivy, 2 * plan.orders.lmax, 2 * plan.orders.mmax, 0, cfg.yflip_offset,
+                       out, scratch, self.scratch_bytes, st)
+            d = self._desc(server, base)
+            d.d_status = slot.status.data_ptr()
+            L.call("euv_amp", C.byref(d), base + self.spec_off, base + self.ax_off, scratch,
+                   self.scratch_bytes, st)
+            imgs = work[self.img_off:self.img_off + self.img_count * 8]
+            imgs.zero_()
+            o = self.table_offsets
+            for (plan, tb, rs), (u0, nu), (ioff, isz), c0 in zip(
+                    self.parts, self.part_units, self.part_images, self.part_clip0):
+                cfg = plan.cfg
+                a = L.AbbeDesc()
+                a.xdiv, a.ydiv, a.lpx, a.lpy = cfg.xdiv, cfg.ydiv, cfg.lpmaxX, cfg.lpmaxY
+                a.ncut, a.n_units, a.n_src, a.n_order = plan.ncut, nu, server.n_src_pad, self.N
+                a.d_coef, a.d_nidx = tb["coef"].data_ptr(), tb["nidx"].data_ptr()
+                a.d_px, a.d_py, a.d_row_start = (tb["px"].data_ptr(), tb["py"].data_ptr(),
+                                                 tb["row_start"].data_ptr())
+                a.d_tab_of_unit = base + o[8] + 4 * u0
+                a.d_img_of_unit = base + o[9] + 4 * u0
+                a.d_nsrc_of_unit = base + o[10] + 4 * u0
+                a.n_images = len(rs) * self.npol
+                a.d_inv_weight = base + o[11] + 8 * c0 * self.npol
+                a.precision = plan.precision
+                L.call("euv_abbe", C.byref(a), base + self.ax_off + u0 * server.n_src_pad * self.N * 16,
+                       base + self.img_off + 8 * ioff, st)
+            slot.hout[:self.img_count].copy_(imgs.view(torch.float64), non_blocking=True)
+            # the launch's device status word travels with its images, then restarts at 0
+            slot.hstat.copy_(slot.status, non_blocking=True)
+            slot.status.zero_()
+            ev = torch.cuda.Event()
+            ev.record(slot.stream)
+        return ev
+
+    def results(self, slot: Slot):
+        """(request, image [pols, xdiv, ydiv]) pairs from the slot's output."""
+        out = slot.hout.numpy()
+        for (plan, _, rs), (ioff, isz) in zip(self.parts, self.part_images):
+            shp = (self.npol, plan.cfg.xdiv, plan.cfg.ydiv)
+            for j, r in enumerate(rs):
+                yield r, out[ioff + j * isz:ioff + (j + 1) * isz].reshape(shp).copy()
+
+
 class Server:
-    def __init__(self, device=None, precision: str = "mixed", max_batch: int = 4,
-                 n_streams: int = 4, hbm_budget: Optional[int] = None, plain: bool = False):
+    """Continuous-batching server.  Mixed precision: requests of one group
+    (order box and polarisations, any period and source count) share a launch:
+    one batched ampS of all their units, then one Abbe launch per
+    configuration.  plain=True: the unbatched FP64 form, one unit per call."""
+
+    def __init__(self, device=None, precision: str = "mixed", max_batch: int = 8,
+                 n_streams: int = 4, hbm_budget: Optional[int] = None, plain: bool = False,
+                 n_src_pad: int = MAX_SOURCES):
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         self.precision = precision
         self.max_batch = 1 if plain else max_batch
         self.plain = plain
-        self.streams = [torch.cuda.Stream(device=self.device) for _ in range(1 if plain else n_streams)]
+        self.n_src_pad = int(n_src_pad)
+        n = 1 if plain else n_streams
+        self.slots = [Slot(self.device) for _ in range(n)]
+        self.streams = [s.stream for s in self.slots]
         free, _ = torch.cuda.mem_get_info(self.device)
         budget = int(hbm_budget if hbm_budget is not None else 0.5 * free)
         self.arena = Arena(budget, self.device)
         self.plans: Dict[ClipKey, Plan] = {}
         self.execs: Dict[Tuple[ClipKey, int], Executor] = {}
+        self.euler: Dict[GroupKey, int] = {}
         self.waits_for_memory = 0
 
     # ---------------------------------------------------------------- set-up
@@ -183,12 +422,35 @@ class Server:
             with torch.cuda.device(self.device):
                 p = Plan(config_for(key), device=self.device, pols=key.pols,
                          precision="fp64" if self.plain else self.precision)
-                p.abbe_tables()
+                p.abbe_tables() if self.plain else p.abbe_tables(self.n_src_pad)
             self.plans[key] = p
         return p
 
+    def _key_euler(self, key: ClipKey) -> int:
+        """Euler factor count ampS derives for this configuration alone."""
+        plan = self.plan(key)
+        tb = plan.abbe_tables(self.n_src_pad)
+        d = plan.amp_desc(plan.orders, plan._t_l, plan._t_m, torch.zeros(1, dtype=torch.float64),
+                          torch.zeros(1, dtype=torch.float64), torch.zeros(1, dtype=torch.int32),
+                          torch.zeros(1, dtype=torch.int32), torch.zeros((1, 1), dtype=torch.int32),
+                          torch.zeros((1, 1), dtype=torch.float64), [])
+        d.k0_max = float(max(np.abs(tb["kx0"]).max(), np.abs(tb["ky0"]).max()))
+        f = L.lib().euv_amp_euler_factors(C.byref(d))
+        if f < -1:
+            raise ValueError("invalid ampS descriptor for %s" % (key,))
+        return f
+
+    def group_euler(self, group: GroupKey) -> int:
+        """The group's fixed Euler factor count: the largest any of its warmed
+        configurations needs alone (the FP64 LU, -1, if one needs it), so a
+        clip's result does not depend on the clips it shares a launch with."""
+        if group not in self.euler:
+            fs = [self._key_euler(k) for k in self.plans if group_of(k) == group]
+            self.euler[group] = -1 if (not fs or -1 in fs) else max(fs)
+        return self.euler[group]
+
     def batch_sizes(self) -> List[int]:
-        """Prepared batch sizes: powers of two up to max_batch."""
+        """Prepared batch sizes of the plain form: powers of two up to max_batch."""
         out, n = [], 1
         while n <= self.max_batch:
             out.append(n)
@@ -200,7 +462,7 @@ class Server:
         if ex is None:
             plan = self.plan(key)
             N = plan.orders.n
-            per_unit = 12 * N * N * 16 + (2 * 4 * N * (N + 16) * 4 if plan.precision == L.EUV_PREC_MIXED else 0)
+            per_unit = 12 * N * N * 16
             # a launch may use at most half of the arena, so two always fit
             max_units = max(1, (self.arena.size // 2) // max(per_unit, 1))
             with torch.cuda.device(self.device):
@@ -212,82 +474,103 @@ class Server:
         return ex
 
     def warm(self, keys: Sequence[ClipKey]) -> None:
-        """Resident tables and prepared batches of every configuration the stream
-        will use (outside any timing)."""
+        """Resident tables of every configuration the stream will use, the
+        groups' Euler factor counts and, for the plain form, prepared batches
+        (outside any timing)."""
         for k in keys:
-            for n in self.batch_sizes():
-                self.executor(k, n)
+            self.plan(k)
+        if self.plain:
+            for k in keys:
+                for n in self.batch_sizes():
+                    self.executor(k, n)
+        else:
+            self.euler.clear()
+            for g in {group_of(k) for k in keys}:
+                self.group_euler(g)
         torch.cuda.synchronize(self.device)
 
     @property
     def resident_bytes(self) -> int:
-        return sum(e.bytes for e in self.execs.values())
+        n = sum(e.bytes for e in self.execs.values())
+        for p in self.plans.values():
+            for tb in (p._abbe_tables or {}).values():
+                n += sum(v.numel() * v.element_size() for v in tb.values()
+                         if isinstance(v, torch.Tensor))
+        return n
 
     # ---------------------------------------------------------------- serve
+    def _take(self, q: Deque[Request]) -> List[Request]:
+        """Up to max_batch of the oldest requests of a group whose launch fits
+        in half of the arena."""
+        rs = [q[0]]
+        while len(rs) < min(self.max_batch, len(q)):
+            trial = GroupLaunch(self, group_of(q[0].key), rs + [q[len(rs)]])
+            if trial.need > self.arena.size // 2:
+                break
+            rs.append(q[len(rs)])
+        for _ in rs:
+            q.popleft()
+        return rs
+
     def serve(self, requests: Sequence[Request]) -> Dict:
         """Run the arrival trace (request.arrival: seconds from now) to completion;
         returns latency and throughput statistics."""
+        if self.plain:
+            return self._serve_plain(requests)
         reqs = sorted(requests, key=lambda r: r.arrival)
-        pending: Dict[ClipKey, Deque[Request]] = collections.defaultdict(collections.deque)
-        inflight = []  # (slot, executor, requests, event, arena offset)
-        free_slots = list(range(len(self.streams)))
+        pending: Dict[GroupKey, Deque[Request]] = collections.defaultdict(collections.deque)
+        inflight = []  # (slot index, launch, event, arena offset)
+        free_slots = list(range(len(self.slots)))
         nxt = 0
         t0 = time.perf_counter()
-        batches = 0
-        clips = 0
-        failed = 0
+        batches = clips = failed = 0
         while nxt < len(reqs) or inflight or any(pending.values()):
             now = time.perf_counter() - t0
             while nxt < len(reqs) and reqs[nxt].arrival <= now:
-                pending[reqs[nxt].key].append(reqs[nxt])
+                pending[group_of(reqs[nxt].key)].append(reqs[nxt])
                 nxt += 1
             still = []
-            for slot, ex, rs, ev, off in inflight:
+            for si, gl, ev, off in inflight:
                 if ev.query():
                     t = time.perf_counter() - t0
-                    img = ex.hout.numpy()
-                    err = L.status_message(int(ex.hstat[0]))
-                    for i, r in enumerate(rs):
-                        r.image = None if err else img[i].copy()
+                    slot = self.slots[si]
+                    err = L.status_message(int(slot.hstat[0]))
+                    for r, img in gl.results(slot):
+                        r.image = None if err else img
                         r.error = err
                         r.done = t
-                    failed += len(rs) if err else 0
-                    ex.busy = False
+                    failed += len(gl.reqs) if err else 0
                     self.arena.free(off)
-                    free_slots.append(slot)
+                    free_slots.append(si)
                 else:
-                    still.append((slot, ex, rs, ev, off))
+                    still.append((si, gl, ev, off))
             inflight = still
             launched = False
             while free_slots:
-                keys = [k for k, q in pending.items() if q]
-                if not keys:
+                groups = [g for g, q in pending.items() if q]
+                if not groups:
                     break
-                key = min(keys, key=lambda k: pending[k][0].arrival)  # oldest request first
-                q = pending[key]
-                sizes = [s for s in self.batch_sizes() if s <= len(q)]
-                ex = None
-                for n in sorted(sizes, reverse=True):
-                    e = self.executor(key, n)
-                    if not e.busy:
-                        ex = e
-                        break
-                if ex is None:
-                    break
-                off = self.arena.alloc(ex.need)
+                g = min(groups, key=lambda k: pending[k][0].arrival)  # oldest request first
+                q = pending[g]
+                rs = self._take(q)
+                gl = GroupLaunch(self, g, rs)
+                off = self.arena.alloc(gl.need)
                 if off is None:  # HBM footprint: wait for a running batch to finish
+                    for r in reversed(rs):
+                        q.appendleft(r)
                     self.waits_for_memory += 1
                     break
-                rs = [q.popleft() for _ in range(ex.n)]
-                slot = free_slots.pop()
-                ex.busy = True
-                ev = ex.launch(rs, self.streams[slot], self.arena.view(off, ex.need))
-                inflight.append((slot, ex, rs, ev, off))
+                si = free_slots.pop()
+                ev = gl.launch(self, self.slots[si], self.arena.view(off, gl.need))
+                inflight.append((si, gl, ev, off))
                 batches += 1
-                clips += ex.n
+                clips += len(rs)
                 launched = True
             if not launched:
                 time.sleep(0.0002)
+        return self._stats(reqs, t0, batches, clips, failed)
+
+    def _stats(self, reqs, t0, batches, clips, failed) -> Dict:
         end = time.perf_counter() - t0
         lat = np.array([r.latency for r in reqs])
         first = min(r.arrival for r in reqs)
@@ -304,6 +587,44 @@ class Server:
             "waits_for_memory": self.waits_for_memory,
             "failed": failed,
         }
+
+    def _serve_plain(self, requests: Sequence[Request]) -> Dict:
+        """The unbatched FP64 form: one request per launch, one unit per ampS call."""
+        reqs = sorted(requests, key=lambda r: r.arrival)
+        pending: Deque[Request] = collections.deque()
+        inflight = None
+        nxt = 0
+        t0 = time.perf_counter()
+        batches = failed = 0
+        stream = self.slots[0].stream
+        while nxt < len(reqs) or inflight or pending:
+            now = time.perf_counter() - t0
+            while nxt < len(reqs) and reqs[nxt].arrival <= now:
+                pending.append(reqs[nxt])
+                nxt += 1
+            if inflight is not None and inflight[2].query():
+                ex, r, ev, off = inflight[0], inflight[1], inflight[2], inflight[3]
+                err = L.status_message(int(ex.hstat[0]))
+                r.image = None if err else ex.hout.numpy()[0].copy()
+                r.error = err
+                r.done = time.perf_counter() - t0
+                failed += 1 if err else 0
+                ex.busy = False
+                self.arena.free(off)
+                inflight = None
+            if inflight is None and pending:
+                r = pending.popleft()
+                ex = self.executor(r.key, 1)
+                off = self.arena.alloc(ex.need)
+                if off is None:
+                    raise MemoryError("the arena cannot hold one plain launch")
+                ex.busy = True
+                ev = ex.launch([r], stream, self.arena.view(off, ex.need))
+                inflight = (ex, r, ev, off)
+                batches += 1
+            else:
+                time.sleep(0.0002)
+        return self._stats(reqs, t0, batches, batches, failed)
 
 
 # -------------------------------------------------------------------- workload

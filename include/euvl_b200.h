@@ -252,9 +252,23 @@ typedef struct {
   int m_max;             /* upper bound on double-angle steps; <= 0: derived */
   double k0_max;         /* bound on |kx0|, |ky0| over the units (<= 0: k) */
   int* d_status;         /* optional device int: EUV_STATUS_* bits OR-ed in (NULL: none) */
+  const double* d_dx;    /* optional [U] clip period of each unit (nm), so that clips of
+                            different periods with the same order set share a launch;
+                            NULL: dx for every unit.  With it, dx must be the smallest
+                            period over the units (it bounds the matrix norms) */
+  const double* d_dy;    /* optional [U], as d_dx */
+  int euler_f;           /* EUV_PREC_MIXED: factors of the Euler product that inverts the
+                            interface matrix (1..8); 0: derived from dx, dy and k0_max so
+                            that the truncation is <= 1e-7; -1: an FP64 LU instead.  Fix it
+                            to make a unit's result independent of the other units of the
+                            launch (the derived count depends on the smallest period) */
 } euv_amp_desc;
 
 size_t euv_amp_workspace_bytes(const euv_amp_desc* desc);
+/* The Euler factor count a launch with this descriptor uses (the euler_f
+ * rule above): 1..8, -1 for the FP64 LU, 0 for EUV_PREC_FP64 (the LU always);
+ * -2 for an invalid descriptor.  Host only. */
+int euv_amp_euler_factors(const euv_amp_desc* desc);
 int euv_amp(const euv_amp_desc* desc, const euv_c64* d_spectra, euv_c64* d_ax, void* d_work,
             size_t work_bytes, void* stream);
 
@@ -514,6 +528,20 @@ int euv_zgemm_tf32x3(int m, int n, int k, euv_c64 alpha, const double* d_scale,
                      long long stride_b, euv_c64 beta, euv_c64* d_c, int ldc, long long stride_c,
                      euv_c64 diag, int batch, const int* d_steps, int step, void* d_work,
                      size_t work_bytes, int* d_status, void* stream);
+
+/* Tuning table: per problem shape, a pick that overrides a kernel's built-in
+ * choice (no reference counterpart; the reference's library calls tune
+ * themselves).  The autotuner (euvlitho_b200.autotune) times the candidates
+ * on the device and writes its picks here; value 0 clears an entry, get
+ * returns 0 when there is none.  Process-wide, all devices. */
+#define EUV_KNOB_ABBE_SPLIT 1 /* key (n_units, n_src) of euv_abbe: CTAs sharing a unit's
+                                 sources, 1..64 (built in: fills the waves of resident CTAs) */
+#define EUV_KNOB_LU_CLUSTER 2 /* key (n, batch) of the LU: smallest CTA cluster of a panel,
+                                 1, 2, 4 or 8 (built in: the fewest CTAs that hold the rows) */
+#define EUV_KNOB_ZGEMM_ROWS 3 /* key (m, batch) of the FP64 GEMM: row tile 64 or 32 */
+int euv_tune_set(int knob, int k0, int k1, int value);
+int euv_tune_get(int knob, int k0, int k1);
+void euv_tune_clear(void);
 
 /* One device thread waits until *d_flag != 0, with the bounded spin that every
  * device wait of the library uses (limit_ns, at most 2e9); on expiry it ORs

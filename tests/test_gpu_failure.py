@@ -76,8 +76,7 @@ def test_served_requests_carry_the_failure_instead_of_an_image(cuda):
     srv = S.Server(device=cuda, precision="mixed", max_batch=1, n_streams=1)
     key = reqs[0].key
     srv.warm([key])
-    ex = srv.executor(key, 1)
-    ex.batch.status.fill_(L.EUV_STATUS_TIMEOUT)  # the next launch of this executor fails
+    srv.slots[0].status.fill_(L.EUV_STATUS_TIMEOUT)  # the next launch of this slot fails
     stats = srv.serve(reqs)
     assert stats["failed"] == 1
     bad = [r for r in reqs if r.error is not None]

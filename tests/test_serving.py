@@ -28,14 +28,32 @@ def test_config_for_gives_the_requested_source_count():
 
 @pytest.mark.gpu
 def test_each_result_same_alone_and_in_the_mix(cuda):
+    """Requests of two periods and two source counts with the same order box
+    share launches (one ampS of all their units, each with its own period);
+    every request's image equals the image the server returns for that clip
+    served alone (1e-13: the launch's other clips do not reach a clip's
+    result), and the engine's own single-configuration image to 1e-5 (the
+    group fixes the Euler factor count of the mixed form, which the engine
+    derives per configuration: the two differ by the product's truncation,
+    below 1e-7 of G^-1)."""
     import torch
-    reqs = S.workload(24, rate=400.0, seed=5, periods=(256, 512), boxes=(5,), source_counts=(50,))
-    srv = S.Server(device=cuda, precision="mixed", max_batch=4, n_streams=3)
-    srv.warm(sorted({r.key for r in reqs}, key=lambda k: (k.period, k.box, k.n_src)))
+    reqs = S.workload(24, rate=400.0, seed=5, periods=(256, 512), boxes=(5,),
+                      source_counts=(50, 100))
+    assert len({r.key for r in reqs}) > 1
+    keys = sorted({r.key for r in reqs}, key=lambda k: (k.period, k.box, k.n_src))
+    srv = S.Server(device=cuda, precision="mixed", max_batch=8, n_streams=3)
+    srv.warm(keys)
     stats = srv.serve(reqs)
-    assert stats["requests"] == len(reqs) and stats["mean_batch"] > 1.0
+    assert stats["requests"] == len(reqs) and stats["failed"] == 0
+    assert stats["mean_batch"] > 1.5
+    alone_srv = S.Server(device=cuda, precision="mixed", max_batch=1, n_streams=1)
+    alone_srv.warm(keys)
     for r in reqs:
+        one = S.Request(r.rid, r.key, r.mask, 0.0)
+        alone_srv.serve([one])
+        err = np.max(np.abs(r.image - one.image)) / np.max(np.abs(one.image))
+        assert err < 1e-13, (r.rid, err)
         plan = srv.plan(r.key)
-        alone = plan.intensity(torch.from_numpy(r.mask[None])).cpu().numpy()[0]
-        err = np.max(np.abs(r.image - alone)) / np.max(np.abs(alone))
-        assert err < 1e-12, (r.rid, err)
+        eng = plan.intensity(torch.from_numpy(r.mask[None])).cpu().numpy()[0]
+        err = np.max(np.abs(r.image - eng)) / np.max(np.abs(eng))
+        assert err < 1e-5, (r.rid, err)
