@@ -48,6 +48,9 @@ def _args():
                     help="skip timing the reference's cuSOLVER/cuBLAS/cuFFT sequence")
     ap.add_argument("--no-served", action="store_true",
                     help="skip the served-form leg (Poisson stream, mixed vs plain FP64)")
+    ap.add_argument("--split-units", action="store_true",
+                    help="N>1: every rank takes a share of the same clips' units and one "
+                         "all-reduce sums the images (strong scaling) instead of replicas")
     return ap.parse_args()
 
 
@@ -406,6 +409,56 @@ class Clocks:
 
 
 # ---------------------------------------------------------------- GPU
+def run_split_units(a, plan, cfg, dev, rank: int, world: int, local: int) -> int:
+    """Strong scaling of one step: all ranks take the same CLIPS clips, rank r
+    solves and images its range of the (clip, polarisation, family) units
+    (engine.unit_range) and an all-reduce (sum) of the FP64 images finishes
+    the step.  Eager launches; the max over ranks of the device time."""
+    import torch
+    import torch.distributed as dist
+    from euvlitho_b200 import masks as MK
+    from euvlitho_b200.engine import unit_range
+    b = plan.intensity_batch(CLIPS)
+    b.masks.copy_(torch.from_numpy(MK.batch(cfg.ndivx, cfg.ndivy, rank_seeds(0, CLIPS))))
+    u0, u1 = unit_range(b.U, world, rank)
+
+    def step():
+        b.run_units(u0, u1)
+        dist.all_reduce(b.image)
+
+    for _ in range(max(a.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks = Clocks(local)
+    clocks.start()
+    dist.barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(a.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    dist.barrier()
+    clk = clocks.stop()
+    ms = max_over_ranks_on(e0.elapsed_time(e1) / a.steps, world, dev)
+    b.check()
+    out = {"metric": METRIC, "value": CLIPS / (ms / 1000.0), "unit": "clips/s", "n_gpus": world,
+           "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True,
+           "scaling": "strong", "vs_baseline": None,
+           "dtype": "f64" if a.precision == "fp64" else "tf32x3+f64",
+           "data": "synthetic (seeded lines+contacts masks, 36% absorber)",
+           "config": {"workload": WORKLOAD, "clips_per_step": CLIPS, "precision": a.precision,
+                      "units_per_step": b.U, "orders": plan.orders.n,
+                      "parallelism": "units split over %d GPUs + all-reduce of the images" % world,
+                      "cuda_graph": False},
+           "clocks": clk}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    return 0
+
+
 def main() -> int:
     a = _args()
     if a.impl == "reference":
@@ -437,6 +490,10 @@ def main() -> int:
 
     cfg = preset("batched")
     plan = Plan(cfg, device=dev, pols=("X", "Y"), precision=a.precision)
+    if a.split_units and world > 1:
+        rc = run_split_units(a, plan, cfg, dev, rank, world, local)
+        dist.destroy_process_group()
+        return rc
     host = MK.batch(cfg.ndivx, cfg.ndivy, rank_seeds(rank, CLIPS))
     b = plan.intensity_batch(CLIPS)
     b.masks.copy_(torch.from_numpy(host))

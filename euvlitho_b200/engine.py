@@ -583,6 +583,19 @@ class Plan:
         return img.real
 
 
+def unit_range(n_units: int, world: int, rank: int) -> Tuple[int, int]:
+    """Units [u0, u1) of ``rank`` when a step's (clip, polarisation, family)
+    units are split over ``world`` GPUs: contiguous ranges whose sizes differ
+    by at most one.  The units are independent until the image sum, so each
+    rank solves and images its range and one all-reduce (sum) of the images
+    finishes the step."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError("rank %d of world %d" % (rank, world))
+    base, extra = divmod(n_units, world)
+    u0 = rank * base + min(rank, extra)
+    return u0, u0 + base + (1 if rank < extra else 0)
+
+
 def _check_word(word: torch.Tensor, where: str) -> None:
     bits = int(word.item())
     if bits:
@@ -662,14 +675,16 @@ class IntensityBatch:
                      else None)
         self.graph: Optional[torch.cuda.CUDAGraph] = None
         self._plain = None
+        self._ranges: Dict[Tuple[int, int], tuple] = {}
 
-    def _unit_descs(self, size: int):
-        """ampS / Abbe descriptors for units [u0, u0+size): pointer offsets into
-        the batch's per-unit tables (the C ABI takes plain pointers)."""
+    def _unit_descs(self, size: int, first: int = 0):
+        """ampS / Abbe descriptors for units [u0, u0+size), u0 = first, first +
+        size, ...: pointer offsets into the batch's per-unit tables (the C ABI
+        takes plain pointers)."""
         out = []
         ns = self.ax.shape[1] * self.ax.shape[2]
         nsrc = self.desc.n_src
-        for u0 in range(0, self.U, size):
+        for u0 in range(first, self.U, size):
             n = min(size, self.U - u0)
             d = L.AmpDesc.from_buffer_copy(self.desc)
             d.n_units = n
@@ -708,6 +723,24 @@ class IntensityBatch:
                    _stream())
         self.image.zero_()
         L.call("euv_abbe", C.byref(self.adesc), self.ax.data_ptr(), self.image.data_ptr(), _stream())
+
+    def run_units(self, u0: int, u1: int, work: Optional[torch.Tensor] = None) -> None:
+        """Spectra, ampS and Abbe of the units [u0, u1) only: the image holds
+        their partial sum (a rank's share of a step split over GPUs; the
+        all-reduce of the partial images is the caller's)."""
+        if not 0 <= u0 <= u1 <= self.U:
+            raise ValueError("unit range [%d, %d) outside [0, %d)" % (u0, u1, self.U))
+        w = self.work if work is None else work
+        self._spectra(w)
+        self.image.zero_()
+        if u1 == u0:
+            return
+        key = (u0, u1)
+        if key not in self._ranges:
+            self._ranges[key] = self._unit_descs(u1 - u0, first=u0)[0]
+        d, a, axp, wb = self._ranges[key]
+        L.call("euv_amp", C.byref(d), self.spec.data_ptr(), axp, w.data_ptr(), w.numel(), _stream())
+        L.call("euv_abbe", C.byref(a), axp, self.image.data_ptr(), _stream())
 
     def run_plain(self, work: Optional[torch.Tensor] = None) -> None:
         """The unbatched FP64 form: every unit solved and imaged on its own."""
