@@ -16,22 +16,17 @@
 // functions tolerate it (intensity error < 1e-4, see the tests); the interface
 // solves stay FP64.
 //
-// The FP64 operands are read straight from global memory by eight converter
-// warps, which split them in registers and store the four fp32 planes of a
-// K-block (Re_hi, Re_lo, Im_hi, Im_lo) into the shared-memory stage in the
-// 64-byte-swizzled K-major layout the UMMA descriptors read -- no operand
-// copies in HBM.  Per CTA (one 128x128 complex tile of C):
-//   warp 0     : TMEM allocation (512 columns: four 128-column accumulators of
-//                the tile) and the single-thread MMA issue loop;
-//   warps 1..8 : converters (ring of 3 stages of 4x(128x16) A + 4x(128x16) B
-//                fp32 = 64 KB), then the epilogue: tcgen05.ld of their TMEM
-//                lane quarter (= 32 rows) over half of the columns, complex
+// Operands are first rewritten (split_*_kernel) as four fp32 planes
+// [batch][Re_hi, Re_lo, Im_hi, Im_lo][rows][Kp] with K contiguous (K-major for
+// both A and B), Kp = K rounded up to 16.  The GEMM kernel:
+//   warp 0     : TMA producer (3-D tensor maps, 64-byte swizzle, 3 stages of
+//                4x(128x16) A + 4x(128x16) B fp32 = 64 KB);
+//   warp 1     : TMEM allocation (512 columns: four 128-column accumulators of
+//                a 128x128 tile) and the single-thread MMA issue loop;
+//   warps 2..5 : epilogue, tcgen05.ld of their 32 TMEM lanes (= rows), complex
 //                FP64 result written column by column (coalesced).
-// C must not overlap A or B (the host checks): other CTAs still read A and B
-// while a tile of C is written.
 // All waits are bounded (about 2 s); a timeout ORs EUV_STATUS_TIMEOUT into the
-// status word, stops the other roles, drains the MMAs in flight, frees TMEM
-// and returns.
+// status word, drains the copies and MMAs in flight, frees TMEM and returns.
 #include "tcgen05.cuh"
 
 namespace euv {
@@ -49,24 +44,19 @@ constexpr int MX_PLANES = 4;
 constexpr int MX_A_TILE = MX_BM * MX_BK * 4;  // 8 KB
 constexpr int MX_B_TILE = MX_BN * MX_BK * 4;  // 8 KB
 constexpr int MX_STAGE_BYTES = MX_PLANES * (MX_A_TILE + MX_B_TILE);  // 64 KB
-constexpr int MX_CONV_WARPS = 8;
-constexpr int MX_THREADS = 32 * (1 + MX_CONV_WARPS);
+constexpr int MX_THREADS = 192;
 constexpr int MX_TMEM_COLS = 512;
 constexpr size_t MX_SMEM = (size_t)MX_STAGES * MX_STAGE_BYTES + 1024 + 256;
 constexpr unsigned long long MX_TIMEOUT_NS = 2000000000ull;
-// A K-block of one operand tile: 4 groups of 32 rows x 4 chunks of 4 K values
-// = 16 warp items; A and B together 32, four per converter warp.
-constexpr int MX_ITEMS = 2 * (MX_BM / 32) * (MX_BK / 4);
-static_assert(MX_ITEMS % MX_CONV_WARPS == 0, "items per converter warp");
+// stage slot of each B plane (gmem order Re_hi, Re_lo, Im_hi, Im_lo)
+__device__ constexpr int kBSlot[4] = {0, 2, 1, 3};
 
 struct MixedArgs {
-  int m, n, k;
+  int m, n, kp;
   double2 alpha, beta, diag;
   const double* scale;
-  const double2* a;
+  const double2* a;  // original FP64 A (copy mode)
   long long lda, sa;
-  const double2* b;
-  long long ldb, sb;
   double2* c;
   const double2* cin;  // C read by the beta term (c when null)
   long long ldc, sc;
@@ -83,25 +73,9 @@ __device__ __forceinline__ constexpr uint32_t idesc_tf32(bool neg_a) {
   return idesc_tf32_mn(neg_a, MX_BM, MX_BN);
 }
 
-// x (FP64) -> hi + lo, hi = x rounded to TF32 (nearest, ties away from zero,
-// on the fp32 value), lo = the exact fp32 remainder; the tensor core reads lo
-// to TF32 precision.  Together about 22 significant bits, the precision of
-// hi*hi + hi*lo + lo*hi.  The TF32 rounding is integer arithmetic on the fp32
-// bits (add half a TF32 unit, clear the 13 low mantissa bits).
-__device__ __forceinline__ void split_fast(double x, float& hi, float& lo) {
-  const float xf = __double2float_rn(x);
-  hi = __uint_as_float((__float_as_uint(xf) + 0x1000u) & 0xffffe000u);
-  lo = xf - hi;
-}
-
-// Byte offset of the 16-byte chunk c (4 K values) of row r in a 64-byte-row
-// K-major tile with the 64-byte swizzle (chunk bits 4-5 XOR address bits 7-8;
-// tiles are 1024-byte aligned).
-__device__ __forceinline__ uint32_t sw64_off(int r, int c) {
-  return (uint32_t)(r * 64 + ((c ^ ((r >> 1) & 3)) << 4));
-}
-
-__global__ void __launch_bounds__(MX_THREADS, 1) gemm_tf32x3_kernel(MixedArgs p) {
+__global__ void __launch_bounds__(MX_THREADS, 1)
+    gemm_tf32x3_kernel(const __grid_constant__ CUtensorMap tmA,
+                       const __grid_constant__ CUtensorMap tmB, MixedArgs p) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
@@ -148,7 +122,7 @@ __global__ void __launch_bounds__(MX_THREADS, 1) gemm_tf32x3_kernel(MixedArgs p)
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < MX_STAGES; ++s) {
-      mbar_init(&full[s], MX_CONV_WARPS);
+      mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
     mbar_init(accum, 1);
@@ -156,26 +130,59 @@ __global__ void __launch_bounds__(MX_THREADS, 1) gemm_tf32x3_kernel(MixedArgs p)
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
-  if (warp == 0) tmem_alloc(tmem_slot, MX_TMEM_COLS);
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tmem_slot)),
+                 "r"(MX_TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
-  const int nkb = (p.k + MX_BK - 1) / MX_BK;
+  const int nkb = p.kp / MX_BK;
 
   if (warp == 0) {
     if (lane == 0) {
-      // A planes: 0 Re_hi 1 Re_lo 2 Im_hi 3 Im_lo.  B stage slots: 0 Re_hi,
-      // 1 Im_hi, 2 Re_lo, 3 Im_lo ([Br | Bi] of one precision level adjacent:
-      // one N = 256 operand).  The FP32 accumulation in TMEM loses precision in
-      // proportion to the K it runs over (measured: the error is the same for
-      // TF32-exact operands and grows linearly in K), so the K range is split
-      // in two halves with their own Re/Im accumulators, summed in FP64 by the
-      // epilogue.  Products: Re = +ArBr -AiBi, Im = +ArBi +AiBr, each as
-      // hi*hi + hi*lo + lo*hi.  The Ar terms of Re and Im share their A
-      // operand: one MMA of N = 256 against [Br | Bi] writes both accumulators
-      // (Re and Im of a K half are adjacent TMEM columns); the Ai terms differ
-      // in sign and take two N = 128 MMAs each (Re negated).
+      int issued = 0;
+      for (int kb = 0; kb < nkb; ++kb) {
+        const int s = kb % MX_STAGES;
+        const uint32_t ph = (uint32_t)((kb / MX_STAGES) & 1);
+        if (!mbar_wait(&empty[s], ph ^ 1u, abort_flag, p.err)) break;
+        mbar_expect_tx(&full[s], (uint32_t)MX_STAGE_BYTES);
+        const int k0 = kb * MX_BK;
+        for (int pl = 0; pl < MX_PLANES; ++pl)
+          tma_load_3d(a_tile(s, pl), &tmA, k0, m0, b * MX_PLANES + pl, &full[s]);
+        // B planes in the stage as Re_hi, Im_hi, Re_lo, Im_lo: [Br | Bi] of a
+        // precision level are adjacent, one N = 256 operand
+        for (int pl = 0; pl < MX_PLANES; ++pl)
+          tma_load_3d(b_tile(s, kBSlot[pl]), &tmB, k0, n0, b * MX_PLANES + pl, &full[s]);
+        issued = kb + 1;
+      }
+      if (*abort_flag) {
+        // drain this thread's copies in flight (bounded) before the CTA exits
+        for (int kb = (issued > MX_STAGES ? issued - MX_STAGES : 0); kb < issued; ++kb) {
+          const unsigned long long t0 = globaltimer();
+          while (!mbar_try(&full[kb % MX_STAGES], (uint32_t)((kb / MX_STAGES) & 1)) &&
+                 globaltimer() - t0 < MX_TIMEOUT_NS) {
+          }
+        }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      // Planes: 0 Re_hi 1 Re_lo 2 Im_hi 3 Im_lo.  The FP32 accumulation in
+      // TMEM loses precision in proportion to the K it runs over (measured: the
+      // error is the same for TF32-exact operands and grows linearly in K), so
+      // the K range is split in two halves with their own Re/Im accumulators,
+      // summed in FP64 by the epilogue.
+      // Products: Re = +ArBr -AiBi, Im = +ArBi +AiBr, each as hi*hi + hi*lo +
+      // lo*hi.  The Ar terms of Re and Im share their A operand: one MMA of
+      // N = 256 against [Br | Bi] (adjacent in the stage) writes both
+      // accumulators (Re and Im of a K half are adjacent TMEM columns); the Ai
+      // terms differ in sign and take two N = 128 MMAs each (Re negated).
+      // A planes: 0 Re_hi 1 Re_lo 2 Im_hi 3 Im_lo; B stage slots: kBSlot.
       const int ar_a[3] = {0, 0, 1}, ar_b[3] = {0, 2, 0};  // B slot of [Br|Bi] hi / lo
       const int ai_a[3] = {2, 2, 3};
       const int ai_bi[3] = {1, 3, 1}, ai_br[3] = {0, 2, 0};  // slots of Bi / Br
@@ -212,81 +219,8 @@ __global__ void __launch_bounds__(MX_THREADS, 1) gemm_tf32x3_kernel(MixedArgs p)
       umma_commit(accum);  // always: the epilogue / teardown waits on it
     }
   } else {
-    // ---- converters: warp item it (0..31) of a K-block; items < 16 are A
-    // (rows m0 + 32*(it/4) + lane, K chunk it%4), the others B (columns).  Each
-    // lane loads the 4 complex values of its chunk (A: 4 columns, 32 lanes =
-    // 512 contiguous bytes per load; B: 64 contiguous bytes of one column),
-    // splits them and stores one 16-byte chunk per plane.  Every item is
-    // loaded before the first store, so the warp has 16 loads in flight.
-    const int cw = warp - 1;
-    const double2* A = p.a + (long long)b * p.sa;
-    const double2* B = p.b + (long long)b * p.sb;
-    for (int kb = 0; kb < nkb; ++kb) {
-      const int s = kb % MX_STAGES;
-      const uint32_t ph = (uint32_t)((kb / MX_STAGES) & 1);
-      const bool got = mbar_wait(&empty[s], ph ^ 1u, abort_flag, p.err);
-      if (!__all_sync(0xffffffffu, got)) break;
-      const int k0 = kb * MX_BK;
-      double2 v[MX_ITEMS / MX_CONV_WARPS][4];
-#pragma unroll
-      for (int j = 0; j < MX_ITEMS / MX_CONV_WARPS; ++j) {
-        const int it = cw + MX_CONV_WARPS * j;
-        const int c = it & 3;
-        const int row = 32 * ((it & 15) >> 2) + lane;
-        const int kc = k0 + 4 * c;
-        if (it < 16) {
-          const int gm = m0 + row;
-#pragma unroll
-          for (int e = 0; e < 4; ++e)
-            v[j][e] = (gm < p.m && kc + e < p.k) ? __ldg(&A[gm + (long long)(kc + e) * p.lda])
-                                                 : make_double2(0.0, 0.0);
-        } else {
-          const int gn = n0 + row;
-          const double2* col = B + (long long)gn * p.ldb + kc;
-#pragma unroll
-          for (int e = 0; e < 4; ++e)
-            v[j][e] = (gn < p.n && kc + e < p.k) ? __ldg(col + e) : make_double2(0.0, 0.0);
-        }
-      }
-#pragma unroll
-      for (int j = 0; j < MX_ITEMS / MX_CONV_WARPS; ++j) {
-        const int it = cw + MX_CONV_WARPS * j;
-        const int c = it & 3;
-        const int row = 32 * ((it & 15) >> 2) + lane;
-        float4 rh, rl, ih, il;
-        split_fast(v[j][0].x, rh.x, rl.x);
-        split_fast(v[j][1].x, rh.y, rl.y);
-        split_fast(v[j][2].x, rh.z, rl.z);
-        split_fast(v[j][3].x, rh.w, rl.w);
-        split_fast(v[j][0].y, ih.x, il.x);
-        split_fast(v[j][1].y, ih.y, il.y);
-        split_fast(v[j][2].y, ih.z, il.z);
-        split_fast(v[j][3].y, ih.w, il.w);
-        const uint32_t off = sw64_off(row, c);
-        if (it < 16) {
-          *reinterpret_cast<float4*>(a_tile(s, 0) + off) = rh;
-          *reinterpret_cast<float4*>(a_tile(s, 1) + off) = rl;
-          *reinterpret_cast<float4*>(a_tile(s, 2) + off) = ih;
-          *reinterpret_cast<float4*>(a_tile(s, 3) + off) = il;
-        } else {
-          *reinterpret_cast<float4*>(b_tile(s, 0) + off) = rh;
-          *reinterpret_cast<float4*>(b_tile(s, 1) + off) = ih;
-          *reinterpret_cast<float4*>(b_tile(s, 2) + off) = rl;
-          *reinterpret_cast<float4*>(b_tile(s, 3) + off) = il;
-        }
-      }
-      // the generic-proxy stores must be visible to the tensor core (async proxy)
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      __syncwarp();
-      if (lane == 0)
-        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&full[s]))
-                     : "memory");
-    }
-
-    // ---- epilogue: warp w reads TMEM lanes 32*(w%4).. (= tile rows) and
-    // columns [64*h, 64*h + 64), h = 0 for warps 1..4, 1 for warps 5..8
+    // epilogue: warps 2..5 read TMEM lanes (warp % 4) * 32 .. +31 = tile rows
     const int q = warp & 3;
-    const int h = (warp - 1) >> 2;
     const bool waited = mbar_wait(accum, 0u, abort_flag, p.err) && !*abort_flag && nkb > 0;
     const bool ok = __all_sync(0xffffffffu, waited);  // tcgen05.ld below is warp-collective
     tc_fence_after();
@@ -298,7 +232,7 @@ __global__ void __launch_bounds__(MX_THREADS, 1) gemm_tf32x3_kernel(MixedArgs p)
     const double2* Cin = p.cin ? p.cin + (long long)b * p.sc : C;
     const cplx dg = mk(p.diag.x, p.diag.y);
     if (ok) {
-      for (int c0 = 64 * h; c0 < 64 * h + 64; c0 += 16) {
+      for (int c0 = 0; c0 < MX_BN; c0 += 16) {
         if (n0 + c0 >= p.n) break;  // warp-uniform
         uint32_t vr[16], vi[16], cr[16], ci[16];
         const uint32_t lane_addr = ((uint32_t)(q * 32) << 16);
@@ -338,58 +272,146 @@ __global__ void __launch_bounds__(MX_THREADS, 1) gemm_tf32x3_kernel(MixedArgs p)
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 0) {
+  if (warp == 1) {
     tc_fence_after();
-    if (*abort_flag) mbar_drain(accum, 0u, MX_TIMEOUT_NS);  // MMAs in flight finish first
-    tmem_dealloc(tmem, MX_TMEM_COLS);
+    if (*abort_flag) {
+      // the MMAs in flight must finish before their TMEM is released (bounded)
+      const unsigned long long t0 = globaltimer();
+      while (!mbar_try(accum, 0u) && globaltimer() - t0 < MX_TIMEOUT_NS) {
+      }
+    }
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(MX_TMEM_COLS)
+                 : "memory");
   }
 }
 
-// ------------------------------------------------------------------ host
-static bool overlaps(const void* a, size_t na, const void* b, size_t nb) {
-  const uintptr_t x = reinterpret_cast<uintptr_t>(a), y = reinterpret_cast<uintptr_t>(b);
-  return x < y + nb && y < x + na;
-}
-static size_t span_bytes(int rows, int cols, long long ld, long long stride, int batch) {
-  return ((size_t)(batch - 1) * (size_t)stride + (size_t)(cols - 1) * (size_t)ld + (size_t)rows) *
-         sizeof(double2);
+// A (col-major complex M x K) -> planes [b][4][M][Kp], K contiguous (transpose
+// through a 32x32 shared tile).
+__global__ void split_a_kernel(int M, int K, int Kp, const double2* A, long long lda,
+                               long long sa, float* out, const int* steps, int step) {
+  __shared__ double2 tile[32][33];
+  const int b = blockIdx.z;
+  if (steps != nullptr && step >= steps[b]) return;  // inactive entry: the GEMM copies
+  const int m0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
+  A += (long long)b * sa;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  for (int j = ty; j < 32; j += 8) {
+    const int m = m0 + tx, k = k0 + j;
+    tile[j][tx] = (m < M && k < K) ? A[m + (long long)k * lda] : make_double2(0.0, 0.0);
+  }
+  __syncthreads();
+  const long long plane = (long long)M * Kp;
+  float* o = out + (long long)b * MX_PLANES * plane;
+  for (int j = ty; j < 32; j += 8) {
+    const int m = m0 + j, k = k0 + tx;
+    if (m < M && k < Kp) {
+      const double2 v = tile[tx][j];
+      float rh, rl, ih, il;
+      split_tf32(v.x, rh, rl);
+      split_tf32(v.y, ih, il);
+      const long long off = (long long)m * Kp + k;
+      o[off] = rh;
+      o[plane + off] = rl;
+      o[2 * plane + off] = ih;
+      o[3 * plane + off] = il;
+    }
+  }
 }
 
-size_t gemm_mixed_workspace_bytes(int, int, int, int) { return 256; }
+// B (col-major complex K x N) -> planes [b][4][N][Kp], K contiguous.
+__global__ void split_b_kernel(int K, int N, int Kp, const double2* B, long long ldb,
+                               long long sb, float* out, const int* steps, int step) {
+  const int b = blockIdx.y;
+  if (steps != nullptr && step >= steps[b]) return;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)N * Kp) return;
+  const int k = (int)(t % Kp), n = (int)(t / Kp);
+  B += (long long)b * sb;
+  const double2 v = k < K ? B[k + (long long)n * ldb] : make_double2(0.0, 0.0);
+  float rh, rl, ih, il;
+  split_tf32(v.x, rh, rl);
+  split_tf32(v.y, ih, il);
+  const long long plane = (long long)N * Kp;
+  float* o = out + (long long)b * MX_PLANES * plane;
+  o[t] = rh;
+  o[plane + t] = rl;
+  o[2 * plane + t] = ih;
+  o[3 * plane + t] = il;
+}
+
+// ------------------------------------------------------------------ host
+// planes tensor [batch*4][rows][kp] fp32 -> 3-D map (kp, rows, batch*4), box (16, box_rows, 1)
+static int make_map(CUtensorMap* map, float* base, int rows, int kp, int nplanes, int box_rows) {
+  const cuuint64_t dims[3] = {(cuuint64_t)kp, (cuuint64_t)rows, (cuuint64_t)nplanes};
+  const cuuint64_t strides[2] = {(cuuint64_t)kp * 4, (cuuint64_t)kp * 4 * rows};
+  const cuuint32_t box[3] = {(cuuint32_t)MX_BK, (cuuint32_t)box_rows, 1};
+  return make_map_f32(map, base, 3, dims, strides, box);
+}
+
+static inline int round_up(int x, int a) { return (x + a - 1) / a * a; }
+
+size_t gemm_mixed_workspace_bytes(int m, int n, int k, int batch) {
+  const size_t kp = (size_t)round_up(k > 0 ? k : 1, MX_BK);
+  size_t a = (size_t)batch * MX_PLANES * (size_t)m * kp * 4;
+  size_t b = (size_t)batch * MX_PLANES * (size_t)n * kp * 4;
+  a = (a + 1023) & ~(size_t)1023;
+  b = (b + 1023) & ~(size_t)1023;
+  return a + b + 1024;
+}
 
 int gemm_mixed(int m, int n, int k, cplx alpha, const double* scale, const double2* a,
                long long lda, long long sa, const double2* b, long long ldb, long long sb,
                cplx beta, double2* c, long long ldc, long long sc, cplx diag, int batch,
                const int* steps, int step, void* work, size_t work_bytes, int* status,
-               cudaStream_t stream, const double2* cin) {
+               cudaStream_t stream, int reuse, const double2* cin) {
   if (m <= 0 || n <= 0 || batch <= 0) return EUV_OK;
-  if (k <= 0 || batch > 65535) {
+  if (k <= 0 || batch > 65535 || (size_t)batch * MX_PLANES > 0x7fffffff) {
     euv_set_error("gemm_mixed: unsupported shape");
     return EUV_ERR_BAD_ARG;
   }
-  const size_t cspan = span_bytes(m, n, ldc, sc, batch);
-  if (overlaps(c, cspan, a, span_bytes(m, k, lda, sa, batch)) ||
-      overlaps(c, cspan, b, span_bytes(k, n, ldb, sb, batch))) {
-    euv_set_error("gemm_mixed: C overlaps A or B (m=%d n=%d k=%d)", m, n, k);
-    return EUV_ERR_BAD_ARG;
+  const int kp = round_up(k, MX_BK);
+  const size_t need = gemm_mixed_workspace_bytes(m, n, k, batch);
+  if (work == nullptr || work_bytes < need ||
+      (reinterpret_cast<uintptr_t>(work) & 255u) != 0) {
+    euv_set_error("gemm_mixed: workspace too small or misaligned (%zu < %zu)", work_bytes, need);
+    return EUV_ERR_WORKSPACE;
   }
+  char* w = reinterpret_cast<char*>(work);
+  float* pa = reinterpret_cast<float*>(w);
+  size_t abytes = ((size_t)batch * MX_PLANES * (size_t)m * kp * 4 + 1023) & ~(size_t)1023;
+  float* pb = reinterpret_cast<float*>(w + abytes);
+  size_t bbytes = ((size_t)batch * MX_PLANES * (size_t)n * kp * 4 + 1023) & ~(size_t)1023;
   // the caller's sticky status word, else a per-call word in the workspace
   int* err = status;
   if (err == nullptr) {
-    if (work == nullptr || work_bytes < sizeof(int)) {
-      euv_set_error("gemm_mixed: workspace too small (%zu bytes; needs %zu without a status word)",
-                    work_bytes, gemm_mixed_workspace_bytes(m, n, k, batch));
-      return EUV_ERR_WORKSPACE;
-    }
-    err = reinterpret_cast<int*>(work);
+    err = reinterpret_cast<int*>(w + abytes + bbytes);
     EUV_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int), stream));
   }
+  // reuse bit 0 / bit 1: the A / B planes in this workspace are already those
+  // of the operand (the caller's previous call split the same unchanged
+  // matrix in the same role and shape), so the split is skipped
+  if (!(reuse & 1)) {
+    dim3 g((m + 31) / 32, (kp + 31) / 32, batch), t(32, 8);
+    split_a_kernel<<<g, t, 0, stream>>>(m, k, kp, a, lda, sa, pa, steps, step);
+    EUV_LAUNCH_CHECK();
+  }
+  if (!(reuse & 2)) {
+    dim3 gb((unsigned)(((long long)n * kp + 255) / 256), batch);
+    split_b_kernel<<<gb, 256, 0, stream>>>(k, n, kp, b, ldb, sb, pb, steps, step);
+    EUV_LAUNCH_CHECK();
+  }
+  CUtensorMap ta, tb;
+  int rc = make_map(&ta, pa, m, kp, batch * MX_PLANES, MX_BM);
+  if (rc) return rc;
+  rc = make_map(&tb, pb, n, kp, batch * MX_PLANES, MX_BN);
+  if (rc) return rc;
   static int smem_done[64];
   EUV_CUDA_TRY(ensure_smem(gemm_tf32x3_kernel, (int)MX_SMEM, smem_done));
   MixedArgs p;
   p.m = m;
   p.n = n;
-  p.k = k;
+  p.kp = kp;
   p.alpha = make_double2(alpha.x, alpha.y);
   p.beta = make_double2(beta.x, beta.y);
   p.diag = make_double2(diag.x, diag.y);
@@ -397,9 +419,6 @@ int gemm_mixed(int m, int n, int k, cplx alpha, const double* scale, const doubl
   p.a = a;
   p.lda = lda;
   p.sa = sa;
-  p.b = b;
-  p.ldb = ldb;
-  p.sb = sb;
   p.c = c;
   p.cin = cin;
   p.ldc = ldc;
@@ -408,7 +427,7 @@ int gemm_mixed(int m, int n, int k, cplx alpha, const double* scale, const doubl
   p.step = step;
   p.err = err;
   dim3 grid((m + MX_BM - 1) / MX_BM, (n + MX_BN - 1) / MX_BN, batch);
-  gemm_tf32x3_kernel<<<grid, MX_THREADS, MX_SMEM, stream>>>(p);
+  gemm_tf32x3_kernel<<<grid, MX_THREADS, MX_SMEM, stream>>>(ta, tb, p);
   EUV_LAUNCH_CHECK();
   return EUV_OK;
 }
@@ -436,5 +455,5 @@ extern "C" int euv_zgemm_tf32x3(int m, int n, int k, euv_c64 alpha, const double
   return gemm_mixed(m, n, k, fromc(alpha), d_scale, reinterpret_cast<const double2*>(d_a), lda,
                     stride_a, reinterpret_cast<const double2*>(d_b), ldb, stride_b, fromc(beta),
                     reinterpret_cast<double2*>(d_c), ldc, stride_c, fromc(diag), batch, d_steps,
-                    step, d_work, work_bytes, d_status, (cudaStream_t)stream, nullptr);
+                    step, d_work, work_bytes, d_status, (cudaStream_t)stream, 0, nullptr);
 }

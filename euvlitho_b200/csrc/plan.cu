@@ -516,6 +516,18 @@ euv_amp_desc amp_base(const euv_plan* P) {
   return d;
 }
 
+// Workspace size of an ampS descriptor whose per-unit pointers are not set yet:
+// the query validates the descriptor (non-null pointers) but reads none of them.
+size_t amp_bytes(euv_amp_desc d) {
+  static const double dd = 0.0;
+  static const int di = 0;
+  d.d_kx0 = d.d_ky0 = d.d_src_2kz = &dd;
+  d.d_polar = d.d_spec = d.d_src_order = &di;
+  if (!d.d_lindex) d.d_lindex = &di;
+  if (!d.d_mindex) d.d_mindex = &di;
+  return euv_amp_workspace_bytes(&d);
+}
+
 int check_run(const euv_plan* P, const uint8_t* d_masks, int n_clips, int n_mask_slices,
               const void* out, const char* who) {
   if (!P || !P->dev) {
@@ -593,7 +605,7 @@ AmpRegions amp_regions(const euv_plan* P, int n_clips, int n_mask_slices, euv_am
   d.n_units = n_clips;
   d.n_src = (int)nna;
   d.k0_max = P->info.k;
-  r.amp = euv_amp_workspace_bytes(&d);
+  r.amp = euv::amp_bytes(d);
   if (dsc) *dsc = d;
   r.total = r.sp.spec + r.sp.raw + r.units + std::max(r.sp.scratch, r.amp) + 256;
   return r;
@@ -914,7 +926,7 @@ IntensityRegions intensity_regions(const euv_plan* P, int n_clips, int n_mask_sl
   d.n_units = (int)U;
   d.n_src = P->n_src;
   d.k0_max = P->info.k;
-  r.amp = euv_amp_workspace_bytes(&d);
+  r.amp = euv::amp_bytes(d);
   if (dsc) *dsc = d;
   r.total = r.sp.spec + r.sp.raw + r.ax + std::max(r.sp.scratch, r.amp) + 256;
   return r;
@@ -1043,7 +1055,7 @@ M3dRegions m3d_regions(const euv_plan* P, int n_clips, int n_mask_slices) {
   d.k0_max = I.k;
   r.uni_scratch = std::max(euv_mask_spectrum_workspace_bytes(2, c.ndivx, c.ndivy, I.fdivx, I.fdivy,
                                                              lhn, mhn),
-                           euv_amp_workspace_bytes(&d));
+                           euv::amp_bytes(d));
   r.uni_total = r.uni_masks + r.uni_spec + r.uni_scratch + 256;
   r.ax_wide = al((size_t)n_clips * I.n_na_sources * I.n_orders * sizeof(euv_c64));
   r.fmask = al((size_t)n_clips * (2 * I.lpx + 1) * (2 * I.lpy + 1) * sizeof(euv_c64));

@@ -38,7 +38,7 @@ int gemm_mixed(int m, int n, int k, cplx alpha, const double* scale, const doubl
                long long lda, long long sa, const double2* b, long long ldb, long long sb,
                cplx beta, double2* c, long long ldc, long long sc, cplx diag, int batch,
                const int* steps, int step, void* work, size_t work_bytes, int* status,
-               cudaStream_t stream, const double2* cin);
+               cudaStream_t stream, int reuse, const double2* cin);
 size_t gemm_mixed_workspace_bytes(int m, int n, int k, int batch);
 
 // ||A||_1 bound for the degree-8 Taylor step of cos/sin(sqrt(A)): the dropped
@@ -552,6 +552,12 @@ __global__ void flag_singular_kernel(const int* info, int n, int* status) {
 
 // GEMM dispatch by precision (FP64 DMMA, or TF32x3 tcgen05 tensor cores for
 // the bulk products of the mixed form; `status` receives EUV_STATUS_TIMEOUT).
+// Gemm reuse flags (mixed form only): the previous call through the same Gemm
+// split this unchanged operand in the same role and shape, so its TF32 planes
+// in the workspace are current.
+constexpr int kReuseA = 1;
+constexpr int kReuseB = 2;
+
 struct Gemm {
   int precision;
   void* mwork;
@@ -561,11 +567,11 @@ struct Gemm {
   int operator()(int m, int n, int k, cplx alpha, const double* scale, const double2* a,
                  long long lda, long long sa, const double2* b, long long ldb, long long sb,
                  cplx beta, double2* c, long long ldc, long long sc, cplx diag, int batch,
-                 const int* steps = nullptr, int step = 0,
+                 const int* steps = nullptr, int step = 0, int reuse = 0,
                  const double2* cin = nullptr) const {
     if (precision == EUV_PREC_MIXED)
       return gemm_mixed(m, n, k, alpha, scale, a, lda, sa, b, ldb, sb, beta, c, ldc, sc, diag,
-                        batch, steps, step, mwork, mbytes, status, stream, cin);
+                        batch, steps, step, mwork, mbytes, status, stream, reuse, cin);
     if (cin != nullptr && cin != c) {
       // FP64 GEMM: the beta term reads C, so C = Cin first (same shape)
       const size_t span = (size_t)(batch - 1) * sc + (size_t)(n - 1) * ldc + m;
@@ -603,17 +609,18 @@ int matfun(int n, int batch, const double2* D, const double* thick, double2** pc
   int rc;
   // P2 = h^4 D D, P3 = h^2 P2 D, P4 = P2 P2
   if ((rc = gemm(n, n, n, one, w.h4, D, n, nn, D, n, nn, zero, w.P2, n, nn, zero, batch))) return rc;
-  if ((rc = gemm(n, n, n, one, w.h2, w.P2, n, nn, D, n, nn, zero, w.P3, n, nn, zero, batch))) return rc;
-  if ((rc = gemm(n, n, n, one, nullptr, w.P2, n, nn, w.P2, n, nn, zero, w.P4, n, nn, zero, batch)))
-    return rc;
+  if ((rc = gemm(n, n, n, one, w.h2, w.P2, n, nn, D, n, nn, zero, w.P3, n, nn, zero, batch, nullptr, 0,
+                 kReuseB))) return rc;  // D as B again
+  if ((rc = gemm(n, n, n, one, nullptr, w.P2, n, nn, w.P2, n, nn, zero, w.P4, n, nn, zero, batch,
+                 nullptr, 0, kReuseA))) return rc;  // P2 as A again
   double2* C = *pc;
   double2* S = *ps;
   taylor_prep_kernel<<<ge, bs, 0, stream>>>(n, batch, D, w.P2, w.P3, w.P4, w.h, w.h2, C, w.T1, S,
                                             w.T2);
   EUV_LAUNCH_CHECK();
   if ((rc = gemm(n, n, n, one, nullptr, w.P4, n, nn, w.T1, n, nn, one, C, n, nn, zero, batch))) return rc;
-  if ((rc = gemm(n, n, n, one, nullptr, w.P4, n, nn, w.T2, n, nn, one, S, n, nn, zero, batch)))
-    return rc;
+  if ((rc = gemm(n, n, n, one, nullptr, w.P4, n, nn, w.T2, n, nn, one, S, n, nn, zero, batch,
+                 nullptr, 0, kReuseA))) return rc;  // P4 as A again
   // double-angle steps; entries with fewer steps copy through (C = A)
   double2* tS = w.P2;
   double2* tC = w.P3;
@@ -622,7 +629,7 @@ int matfun(int n, int batch, const double2* D, const double* thick, double2** pc
                    batch, w.steps, step)))
       return rc;
     if ((rc = gemm(n, n, n, mk(2.0, 0.0), nullptr, C, n, nn, C, n, nn, zero, tC, n, nn,
-                   mk(-1.0, 0.0), batch, w.steps, step)))
+                   mk(-1.0, 0.0), batch, w.steps, step, kReuseB)))  // C as B again
       return rc;
     double2* t = S;
     S = tS;
@@ -880,19 +887,24 @@ extern "C" int euv_amp(const euv_amp_desc* d, const euv_c64* d_spectra, euv_c64*
                                                       : euler_factors(d);
   // factors f = 1..euler_f-1 applied to the partial product held in Zbuf (the
   // f = 0 factor is applied by the caller); E^(2^f) ping-pongs between G and P2
-  auto euler_tail = [&](double2* Zbuf) -> int {
+  // g_split: the caller's last GEMM had G as its A operand
+  auto euler_tail = [&](double2* Zbuf, bool g_split) -> int {
     double2* P = w.G;
     double2* Pn = w.P2;
     double2* Zc = Zbuf;
     double2* Zt = w.W;
     for (int f = 1; f < euler_f; ++f) {
-      int r2 = gemm(N, N, N, one, nullptr, P, N, nn, P, N, nn, zero, Pn, N, nn, zero, U);
+      // P as A again: split by the previous factor's P Zc (or the caller's G Z)
+      const int ru = (f > 1 || g_split) ? kReuseA : 0;
+      int r2 = gemm(N, N, N, one, nullptr, P, N, nn, P, N, nn, zero, Pn, N, nn, zero, U, nullptr, 0,
+                    ru);
       if (r2) return r2;
       double2* t = P;
       P = Pn;
       Pn = t;
       // Zt = P Zc + Zc (the beta term read from Zc)
-      r2 = gemm(N, N, N, one, nullptr, P, N, nn, Zc, N, nn, one, Zt, N, nn, zero, U, nullptr, 0, Zc);
+      r2 = gemm(N, N, N, one, nullptr, P, N, nn, Zc, N, nn, one, Zt, N, nn, zero, U, nullptr, 0, 0,
+                Zc);
       if (r2) return r2;
       t = Zc;
       Zc = Zt;
@@ -919,7 +931,7 @@ extern "C" int euv_amp(const euv_amp_desc* d, const euv_c64* d_spectra, euv_c64*
       // product on the tensor cores (E was built in place of G)
       euler_first_diag_kernel<<<ge, bs, 0, stream>>>(N, cdiv(one, mk(0.0, d->k)), w.G, w.gx2, w.Z);
       EUV_LAUNCH_CHECK();
-      if ((rc = euler_tail(w.Z))) return rc;
+      if ((rc = euler_tail(w.Z, false))) return rc;
       Zp = w.Z;
     } else if (bottom) {
       // Z = G^-1 diag(Bru (URUU+URUB))
@@ -937,11 +949,11 @@ extern "C" int euv_amp(const euv_amp_desc* d, const euv_c64* d_spectra, euv_c64*
                                              d->d_kx0, d->d_ky0, d->d_polar, nullptr, w.Gp, 0, 2);
       EUV_LAUNCH_CHECK();
       if ((rc = gemm(N, N, N, mk(-1.0, 0.0), nullptr, w.Gp, N, nn, X, N, nn, one, w.Z, N, nn, zero,
-                     U, nullptr, 0, X))) return rc;  // Z = X - Gp X
+                     U, nullptr, 0, 0, X))) return rc;  // Z = X - Gp X
       if ((rc = gemm(N, N, N, one, nullptr, w.G, N, nn, w.Z, N, nn, one, w.W, N, nn, zero, U,
-                     nullptr, 0, w.Z))) return rc;  // W = Z + G Z
+                     nullptr, 0, 0, w.Z))) return rc;  // W = Z + G Z
       EUV_CUDA_TRY(cudaMemcpyAsync(w.Z, w.W, (size_t)U * nn * sizeof(double2), cudaMemcpyDeviceToDevice, stream));
-      if ((rc = euler_tail(w.Z))) return rc;
+      if ((rc = euler_tail(w.Z, true))) return rc;
       Zp = w.Z;
     } else if (d->refresh_sigma) {
       // Z = G_n^-1 G_{n+1} X
@@ -968,9 +980,11 @@ extern "C" int euv_amp(const euv_amp_desc* d, const euv_c64* d_spectra, euv_c64*
     double2* Wb = fr[0];
     double2* Xn = fr[1];
     double2* Yn = fr[2];
-    // W = S Z ; Xn = C Z - i S Y ; Yn = -i D W + C Y
+    // W = S Z ; Xn = C Z - i S Y ; Yn = -i D W + C Y, ordered so that three of
+    // the five products find one operand already split
     if ((rc = gemm(N, N, N, one, nullptr, S, N, nn, Zp, N, nn, zero, Wb, N, nn, zero, U))) return rc;
-    if ((rc = gemm(N, N, N, one, nullptr, C, N, nn, Zp, N, nn, zero, Xn, N, nn, zero, U))) return rc;
+    if ((rc = gemm(N, N, N, one, nullptr, C, N, nn, Zp, N, nn, zero, Xn, N, nn, zero, U, nullptr, 0,
+                   kReuseB))) return rc;  // Zp as B again
     if (bottom) {
       if ((rc = gemm(N, N, N, mi, nullptr, w.D, N, nn, Wb, N, nn, zero, Yn, N, nn, zero, U))) return rc;
       colscale_kernel<<<ge, bs, 0, stream>>>(N, mi, S, w.y2, one, Xn);
@@ -978,8 +992,10 @@ extern "C" int euv_amp(const euv_amp_desc* d, const euv_c64* d_spectra, euv_c64*
       colscale_kernel<<<ge, bs, 0, stream>>>(N, one, C, w.y2, one, Yn);
       EUV_LAUNCH_CHECK();
     } else {
-      if ((rc = gemm(N, N, N, one, nullptr, C, N, nn, Y, N, nn, zero, Yn, N, nn, zero, U))) return rc;
-      if ((rc = gemm(N, N, N, mi, nullptr, S, N, nn, Y, N, nn, one, Xn, N, nn, zero, U))) return rc;
+      if ((rc = gemm(N, N, N, one, nullptr, C, N, nn, Y, N, nn, zero, Yn, N, nn, zero, U, nullptr,
+                     0, kReuseA))) return rc;  // C as A again
+      if ((rc = gemm(N, N, N, mi, nullptr, S, N, nn, Y, N, nn, one, Xn, N, nn, zero, U, nullptr, 0,
+                     kReuseB))) return rc;  // Y as B again
       if ((rc = gemm(N, N, N, mi, nullptr, w.D, N, nn, Wb, N, nn, one, Yn, N, nn, zero, U))) return rc;
     }
     if (n == 0) {

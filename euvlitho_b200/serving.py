@@ -414,6 +414,8 @@ class Server:
         self.execs: Dict[Tuple[ClipKey, int], Executor] = {}
         self.euler: Dict[GroupKey, int] = {}
         self.waits_for_memory = 0
+        # the requests of every grouped launch, in launch order (for inspection)
+        self.launched_groups: List[List[Request]] = []
 
     # ---------------------------------------------------------------- set-up
     def plan(self, key: ClipKey) -> Plan:
@@ -563,6 +565,7 @@ class Server:
                 si = free_slots.pop()
                 ev = gl.launch(self, self.slots[si], self.arena.view(off, gl.need))
                 inflight.append((si, gl, ev, off))
+                self.launched_groups.append(gl.reqs)
                 batches += 1
                 clips += len(rs)
                 launched = True

@@ -516,12 +516,10 @@ int euv_zgemm(int m, int n, int k, euv_c64 alpha, const double* d_scale, const e
 
 /* The bulk product of EUV_PREC_MIXED: same contract as euv_zgemm, computed on
  * the tcgen05 tensor cores as TF32x3 (each FP64 operand split into two TF32
- * terms inside the kernel, three TF32 products per real product, FP32
- * accumulation; ~1e-6 relative error per product).  C must not overlap A or B
- * (EUV_ERR_BAD_ARG).  d_status (optional device int): EUV_STATUS_TIMEOUT is
- * OR-ed in if one of the kernel's bounded waits (about 2 s) gave up; without
- * it the call keeps a per-call status word in d_work (256 bytes,
- * euv_zgemm_tf32x3_workspace_bytes). */
+ * terms, three TF32 products per real product, FP32 accumulation; ~1e-6
+ * relative error per product).  Needs a workspace for the split operands.
+ * d_status (optional device int): EUV_STATUS_TIMEOUT is OR-ed in if one of the
+ * kernel's bounded waits (about 2 s) gave up. */
 size_t euv_zgemm_tf32x3_workspace_bytes(int m, int n, int k, int batch);
 int euv_zgemm_tf32x3(int m, int n, int k, euv_c64 alpha, const double* d_scale,
                      const euv_c64* d_a, int lda, long long stride_a, const euv_c64* d_b, int ldb,

@@ -115,15 +115,3 @@ def test_descriptor_layout_matches_the_header(tmp_path):
         for f, _ in py._fields_:
             assert got[(cname, f)] == getattr(py, f).offset, (cname, f)
 
-
-def test_mixed_gemm_rejects_c_overlapping_an_operand(lib):
-    """The TF32x3 GEMM reads A and B from every CTA while tiles of C are
-    written, so an output that overlaps an operand is refused on the host
-    (addresses only; nothing is launched or dereferenced)."""
-    base = 1 << 20
-    n = 64
-    rc = lib.euv_zgemm_tf32x3(n, n, n, L.c64.of(1), None, base, n, n * n, base + (1 << 22), n,
-                              n * n, L.c64.of(0), base + 16 * n, n, n * n, L.c64.of(0), 1, None, 0,
-                              None, 0, None, None)
-    assert rc == L.EUV_ERR_BAD_ARG
-    assert b"overlaps" in lib.euv_last_error()

@@ -152,3 +152,20 @@ def test_plan_rejects_invalid_configurations(lib, bad):
     assert lib.euv_plan_create(C.byref(c), C.byref(p)) == L.EUV_ERR_BAD_ARG
     assert not p.value
     assert lib.euv_last_error()
+
+
+@pytest.mark.parametrize("name,cfg,pols", CONFIGS[:4], ids=[c[0] for c in CONFIGS[:4]])
+def test_plan_workspaces_hold_the_batched_solve(lib, name, cfg, pols):
+    """The run functions' workspace queries include the batched ampS scratch
+    (twelve N x N complex blocks per unit) on top of spectra and amplitudes."""
+    p, info = _plan(lib, cfg, pols)
+    try:
+        N = info.n_orders
+        for clips in (1, 3):
+            U = clips * info.units_per_clip
+            need = 12 * N * N * 16 * U
+            assert lib.euv_plan_intensity_workspace_bytes(p, clips, 1) > need
+            assert lib.euv_plan_amp_workspace_bytes(p, clips, 1) > 12 * N * N * 16 * clips
+            assert lib.euv_plan_m3d_workspace_bytes(p, clips, 1) > 12 * N * N * 16 * clips
+    finally:
+        lib.euv_plan_destroy(p)

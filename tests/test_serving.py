@@ -37,7 +37,9 @@ def test_each_result_same_alone_and_in_the_mix(cuda):
     derives per configuration: the two differ by the product's truncation,
     below 1e-7 of G^-1)."""
     import torch
-    reqs = S.workload(24, rate=400.0, seed=5, periods=(256, 512), boxes=(5,),
+    # arrivals within a fraction of a millisecond: the requests queue up while
+    # the first launches run, so later launches mix periods and source counts
+    reqs = S.workload(24, rate=1e5, seed=5, periods=(256, 512), boxes=(5,),
                       source_counts=(50, 100))
     assert len({r.key for r in reqs}) > 1
     keys = sorted({r.key for r in reqs}, key=lambda k: (k.period, k.box, k.n_src))
@@ -46,6 +48,7 @@ def test_each_result_same_alone_and_in_the_mix(cuda):
     stats = srv.serve(reqs)
     assert stats["requests"] == len(reqs) and stats["failed"] == 0
     assert stats["mean_batch"] > 1.5
+    assert any(len({r.key for r in gl}) > 1 for gl in srv.launched_groups)
     alone_srv = S.Server(device=cuda, precision="mixed", max_batch=1, n_streams=1)
     alone_srv.warm(keys)
     for r in reqs:
