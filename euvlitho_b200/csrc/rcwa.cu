@@ -751,7 +751,9 @@ static bool carve(const euv_amp_desc* d, Bump& bp, AmpWork& w) {
   w.ipiv = bp.take<int>(U * N);
   w.info = bp.take<int>(U);
   w.capped = bp.take<int>(1);
-  w.mbytes = d->precision == EUV_PREC_MIXED ? gemm_mixed_workspace_bytes((int)N, (int)N, (int)N, (int)U) : 0;
+  // the mixed products are N x N x N, and N x n_src x N for the interface (n_src may exceed N)
+  const int ncol = d->n_src > N ? d->n_src : (int)N;
+  w.mbytes = d->precision == EUV_PREC_MIXED ? gemm_mixed_workspace_bytes((int)N, ncol, (int)N, (int)U) : 0;
   w.mwork = w.mbytes ? bp.take<char>(w.mbytes) : nullptr;
   return bp.ok;
 }
