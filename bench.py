@@ -201,9 +201,10 @@ def dominant_kernel_roofline(plan, U, precision, dev, stream, L):
     Algorithmic work: one complex N x N x N product = 8 N^3 real FLOP per unit
     (the convention for a complex GEMM, whatever the arithmetic that carries
     it out); peak = the measured dense bf16 tensor rate.  Secondary keys give
-    the rate the kernel actually executes: mixed = TF32x3, three TF32 products
-    per real product (24 N^3 TF32 FLOP per unit) against a cuBLAS TF32 GEMM
-    measured in this run; fp64 = DMMA against cuBLAS ZGEMM measured here."""
+    the rate the kernel actually executes: mixed = split-FP16x3, three fp16
+    products per real product (24 N^3 fp16 FLOP per unit, split launches
+    included) against a cuBLAS fp16 GEMM measured in this run; fp64 = DMMA
+    against cuBLAS ZGEMM measured here."""
     import torch
     N = plan.orders.n
     A = torch.randn(U, N, N, dtype=torch.complex128, device=dev)
@@ -212,28 +213,25 @@ def dominant_kernel_roofline(plan, U, precision, dev, stream, L):
     s = stream.cuda_stream
     flop = 8.0 * N ** 3 * U
     if precision == "mixed":
-        wb = L.lib().euv_zgemm_tf32x3_workspace_bytes(N, N, N, U)
+        wb = L.lib().euv_zgemm_mixed_workspace_bytes(N, N, N, U)
         ws = torch.empty(max(wb, 256), dtype=torch.uint8, device=dev)
 
         def gemm():
-            L.call("euv_zgemm_tf32x3", N, N, N, L.c64(1, 0), None, A.data_ptr(), N, N * N,
+            L.call("euv_zgemm_mixed", N, N, N, L.c64(1, 0), None, A.data_ptr(), N, N * N,
                    B.data_ptr(), N, N * N, L.c64(0, 0), C.data_ptr(), N, N * N, L.c64(0, 0), U,
                    None, 0, ws.data_ptr(), wb, None, s)
         ms = _time_ms(gemm, stream, 10)
-        X = torch.randn(8192, 8192, dtype=torch.float32, device=dev)
-        Y = torch.randn(8192, 8192, dtype=torch.float32, device=dev)
-        old = torch.backends.cuda.matmul.allow_tf32
-        torch.backends.cuda.matmul.allow_tf32 = True
-        tf32 = 2.0 * 8192 ** 3 / (_time_ms(lambda: torch.matmul(X, Y), stream, 5) / 1e3) / 1e12
-        torch.backends.cuda.matmul.allow_tf32 = old
+        X = torch.randn(8192, 8192, dtype=torch.float16, device=dev)
+        Y = torch.randn(8192, 8192, dtype=torch.float16, device=dev)
+        f16 = 2.0 * 8192 ** 3 / (_time_ms(lambda: torch.matmul(X, Y), stream, 5) / 1e3) / 1e12
         executed = 24.0 * N ** 3 * U / (ms / 1e3) / 1e12
         out = {"bound": "tensor",
-               "kernel": "gemm_tf32x3_kernel (tcgen05 kind::tf32, TMEM accumulators), batch "
-                         "%d x %d^3 complex" % (U, N),
-               "traffic": _traffic("gemm_tf32x3_n961.json"),
-               "tf32x3_executed_tflops": executed,
-               "cublas_tf32_tflops_in_run": tf32,
-               "frac_of_cublas_tf32": executed / tf32}
+               "kernel": "gemm_split3_kernel (tcgen05 kind::f16, TMEM accumulators) + its split "
+                         "launches, batch %d x %d^3 complex" % (U, N),
+               "traffic": _traffic("gemm_split3_n961.json"),
+               "split3_executed_tflops": executed,
+               "cublas_fp16_tflops_in_run": f16,
+               "frac_of_cublas_fp16": executed / f16}
     else:
         def gemm():
             L.call("euv_zgemm", N, N, N, L.c64(1, 0), None, A.data_ptr(), N, N * N, B.data_ptr(),
@@ -447,7 +445,7 @@ def run_split_units(a, plan, cfg, dev, rank: int, world: int, local: int) -> int
     out = {"metric": METRIC, "value": CLIPS / (ms / 1000.0), "unit": "clips/s", "n_gpus": world,
            "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True,
            "scaling": "strong", "vs_baseline": None,
-           "dtype": "f64" if a.precision == "fp64" else "tf32x3+f64",
+           "dtype": "f64" if a.precision == "fp64" else "f16x3+f64",
            "data": "synthetic (seeded lines+contacts masks, 36% absorber)",
            "config": {"workload": WORKLOAD, "clips_per_step": CLIPS, "precision": a.precision,
                       "units_per_step": b.U, "orders": plan.orders.n,
@@ -643,7 +641,7 @@ def main() -> int:
         "metric": METRIC, "value": value, "unit": "clips/s", "n_gpus": world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64" if a.precision == "fp64" else "tf32x3+f64",
+        "dtype": "f64" if a.precision == "fp64" else "f16x3+f64",
         "data": "synthetic (seeded lines+contacts masks, 36% absorber)",
         "config": {"workload": WORKLOAD, "clips_per_step": CLIPS, "precision": a.precision,
                    "units_per_step": b.U, "orders": plan.orders.n,

@@ -34,7 +34,7 @@ EXPORTS = (
     "euv_mask_spectrum_workspace_bytes", "euv_mask_spectrum",
     "euv_amp_workspace_bytes", "euv_amp", "euv_amp_euler_factors",
     "euv_abbe", "euv_m3d_fit",
-    "euv_zgemm", "euv_zgemm_tf32x3_workspace_bytes", "euv_zgemm_tf32x3", "euv_lu_workspace_bytes", "euv_lu_factor", "euv_lu_solve",
+    "euv_zgemm", "euv_zgemm_mixed_workspace_bytes", "euv_zgemm_mixed", "euv_lu_workspace_bytes", "euv_lu_factor", "euv_lu_solve",
     "euv_matfun_workspace_bytes", "euv_matfun_cs", "euv_matfun_cs_noalloc",
     "euv_wait_probe", "euv_linear_amp", "euv_mask_raster_workspace_bytes", "euv_mask_raster",
     "euv_heev_workspace_bytes", "euv_heev", "euv_socs_workspace_bytes", "euv_socs_image",
@@ -215,10 +215,10 @@ def _declare(lib: C.CDLL) -> None:
     lib.euv_m3d_fit.argtypes = [C.POINTER(M3dDesc), P, P, P, P, P, P]
     lib.euv_zgemm.restype = i
     lib.euv_zgemm.argtypes = [i, i, i, c64, P, P, i, ll, P, i, ll, c64, P, i, ll, c64, i, P, i, P]
-    lib.euv_zgemm_tf32x3_workspace_bytes.restype = sz
-    lib.euv_zgemm_tf32x3_workspace_bytes.argtypes = [i, i, i, i]
-    lib.euv_zgemm_tf32x3.restype = i
-    lib.euv_zgemm_tf32x3.argtypes = [i, i, i, c64, P, P, i, ll, P, i, ll, c64, P, i, ll, c64, i, P, i, P, sz,
+    lib.euv_zgemm_mixed_workspace_bytes.restype = sz
+    lib.euv_zgemm_mixed_workspace_bytes.argtypes = [i, i, i, i]
+    lib.euv_zgemm_mixed.restype = i
+    lib.euv_zgemm_mixed.argtypes = [i, i, i, c64, P, P, i, ll, P, i, ll, c64, P, i, ll, c64, i, P, i, P, sz,
                                      P, P]
     lib.euv_lu_workspace_bytes.restype = sz
     lib.euv_lu_workspace_bytes.argtypes = [i, i]

@@ -15,7 +15,7 @@ Knobs (``EUV_KNOB_*`` in include/euvl_b200.h):
 * ``lu_cluster``  -- key (n, batch) of an LU: the smallest CTA cluster that
   factors a panel (built in: the fewest CTAs whose registers hold its rows);
 * ``zgemm_rows``  -- key (m, batch) of the FP64 GEMM: 64- or 32-row tiles
-  (FP64 form only; the mixed form's products run on the TF32x3 kernel).
+  (FP64 form only; the mixed form's products run on the split-FP16x3 kernel).
 
 The cache file is ``$EUVLITHO_TUNE_CACHE`` or
 ``~/.cache/euvlitho_b200/tuning.json``: ``{gpu name: {"knob/k0/k1": value}}``.

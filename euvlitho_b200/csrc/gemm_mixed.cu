@@ -2,31 +2,41 @@
 //
 // C = alpha*scale[b] * A B + beta C + diag*I for complex FP64 A (MxK), B (KxN),
 // C (MxN), column-major and batched (the beta term may read a separate Cin of
-// C's shape), computed as TF32x3: every FP64 real
-// operand is split into two TF32 values x = hi + lo (hi = x rounded to TF32,
-// lo = x - hi), and each real product is hi*hi + hi*lo + lo*hi with FP32
-// accumulation in tensor memory.  The complex product uses four real products:
+// C's shape), computed as split-FP16x3 with power-of-two scaling: every row of
+// A and every column of B is scaled by 2^e (e from its largest |re|, |im|, so
+// that the scaled values lie below 2^15), each scaled FP64 real is split into
+// two fp16 values x = hi + lo (hi = x rounded to fp16, lo = the remainder
+// rounded to fp16) and each real product is hi*hi + hi*lo + lo*hi with FP32
+// accumulation in tensor memory (kind::f16, twice the TF32 rate); the
+// epilogue multiplies by 2^-(e_row + e_col).  fp16 carries the same 11
+// significant bits as TF32, so the products keep about 22 bits (the scaling
+// only moves the values into fp16's exponent range; entries more than 2^24
+// below their row's or column's largest lose relative precision but add at
+// most 2^-38 of it to a product).  The complex product uses four real products:
 //   Re = ArBr - AiBi,  Im = ArBi + AiBr   (the minus sign through the MMA's
-//   negate-A bit): twelve real TF32 products per K=8 step, issued as nine
+//   negate-A bit): twelve real products per K=16 step, issued as nine
 //   tcgen05.mma (the three Ar products as N = 256 against [Br | Bi], writing
-//   the adjacent Re and Im accumulators at once).  The FP32 accumulation error grows with the K it spans, so
-//   the two halves of K have their own Re/Im accumulators (four in all),
-//   summed in FP64 by the epilogue.
+//   the adjacent Re and Im accumulators at once).  The FP32 accumulation error
+//   grows with the K it spans, so the two halves of K have their own Re/Im
+//   accumulators (four in all), summed in FP64 by the epilogue.
 // Error per product ~1e-6 relative: the bulk products of the slab matrix
 // functions tolerate it (intensity error < 1e-4, see the tests); the interface
 // solves stay FP64.
 //
-// Operands are first rewritten (split_*_kernel) as four fp32 planes
-// [batch][Re_hi, Re_lo, Im_hi, Im_lo][rows][Kp] with K contiguous (K-major for
-// both A and B), Kp = K rounded up to 16.  The GEMM kernel:
+// Operands are first rewritten (split_*_kernel: the row or column maxima,
+// then the split) as four fp16 planes [batch][Re_hi, Re_lo, Im_hi, Im_lo]
+// [rows][Kp] with K contiguous (K-major for both A and B), Kp = K rounded up
+// to 32, and the exponents [batch][rows].  The GEMM kernel:
 //   warp 0     : TMA producer (3-D tensor maps, 64-byte swizzle, 3 stages of
-//                4x(128x16) A + 4x(128x16) B fp32 = 64 KB);
+//                4x(128x32) A + 4x(128x32) B fp16 = 64 KB);
 //   warp 1     : TMEM allocation (512 columns: four 128-column accumulators of
 //                a 128x128 tile) and the single-thread MMA issue loop;
 //   warps 2..5 : epilogue, tcgen05.ld of their 32 TMEM lanes (= rows), complex
 //                FP64 result written column by column (coalesced).
 // All waits are bounded (about 2 s); a timeout ORs EUV_STATUS_TIMEOUT into the
 // status word, drains the copies and MMAs in flight, frees TMEM and returns.
+#include <cuda_fp16.h>
+
 #include "tcgen05.cuh"
 
 namespace euv {
@@ -38,11 +48,11 @@ int zgemm(int m, int n, int k, cplx alpha, const double* scale, const double2* a
 
 constexpr int MX_BM = 128;
 constexpr int MX_BN = 128;
-constexpr int MX_BK = 16;  // fp32 elements: 64-byte rows, one 64B swizzle span
+constexpr int MX_BK = 32;  // fp16 elements: 64-byte rows, one 64B swizzle span
 constexpr int MX_STAGES = 3;
 constexpr int MX_PLANES = 4;
-constexpr int MX_A_TILE = MX_BM * MX_BK * 4;  // 8 KB
-constexpr int MX_B_TILE = MX_BN * MX_BK * 4;  // 8 KB
+constexpr int MX_A_TILE = MX_BM * MX_BK * 2;  // 8 KB
+constexpr int MX_B_TILE = MX_BN * MX_BK * 2;  // 8 KB
 constexpr int MX_STAGE_BYTES = MX_PLANES * (MX_A_TILE + MX_B_TILE);  // 64 KB
 constexpr int MX_THREADS = 192;
 constexpr int MX_TMEM_COLS = 512;
@@ -63,18 +73,34 @@ struct MixedArgs {
   const int* steps;
   int step;
   int* err;
+  const int* ea;  // [b][m] power-of-two exponent each row of A was scaled by
+  const int* eb;  // [b][n] the same for the columns of B
 };
 
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
                                           int* err) {
   return mbar_wait_bounded(bar, parity, abort_flag, err, MX_TIMEOUT_NS);
 }
-__device__ __forceinline__ constexpr uint32_t idesc_tf32(bool neg_a) {
-  return idesc_tf32_mn(neg_a, MX_BM, MX_BN);
+// Instruction descriptor of kind::f16: D f32, A and B f16 (format 0), both K-major.
+__host__ __device__ __forceinline__ constexpr uint32_t idesc_f16_mn(bool neg_a, int m, int n) {
+  return (1u << 4) | ((neg_a ? 1u : 0u) << 13) | ((uint32_t)(n >> 3) << 17) |
+         ((uint32_t)(m >> 4) << 24);
+}
+__device__ __forceinline__ constexpr uint32_t idesc_f16(bool neg_a) {
+  return idesc_f16_mn(neg_a, MX_BM, MX_BN);
+}
+__device__ __forceinline__ void umma_f16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc,
+                                         uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(idesc), "r"(accumulate)
+      : "memory");
 }
 
 __global__ void __launch_bounds__(MX_THREADS, 1)
-    gemm_tf32x3_kernel(const __grid_constant__ CUtensorMap tmA,
+    gemm_split3_kernel(const __grid_constant__ CUtensorMap tmA,
                        const __grid_constant__ CUtensorMap tmB, MixedArgs p) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>(
@@ -174,7 +200,7 @@ __global__ void __launch_bounds__(MX_THREADS, 1)
     if (lane == 0) {
       // Planes: 0 Re_hi 1 Re_lo 2 Im_hi 3 Im_lo.  The FP32 accumulation in
       // TMEM loses precision in proportion to the K it runs over (measured: the
-      // error is the same for TF32-exact operands and grows linearly in K), so
+      // error is the same for exactly split operands and grows linearly in K), so
       // the K range is split in two halves with their own Re/Im accumulators,
       // summed in FP64 by the epilogue.
       // Products: Re = +ArBr -AiBi, Im = +ArBi +AiBr, each as hi*hi + hi*lo +
@@ -186,8 +212,8 @@ __global__ void __launch_bounds__(MX_THREADS, 1)
       const int ar_a[3] = {0, 0, 1}, ar_b[3] = {0, 2, 0};  // B slot of [Br|Bi] hi / lo
       const int ai_a[3] = {2, 2, 3};
       const int ai_bi[3] = {1, 3, 1}, ai_br[3] = {0, 2, 0};  // slots of Bi / Br
-      const uint32_t id_pos = idesc_tf32(false), id_neg = idesc_tf32(true);
-      const uint32_t id_wide = idesc_tf32_mn(false, MX_BM, 2 * MX_BN);
+      const uint32_t id_pos = idesc_f16(false), id_neg = idesc_f16(true);
+      const uint32_t id_wide = idesc_f16_mn(false, MX_BM, 2 * MX_BN);
       const int half = (nkb + 1) / 2;  // k-blocks [0, half) -> set 0, [half, nkb) -> set 1
       for (int kb = 0; kb < nkb; ++kb) {
         const int s = kb % MX_STAGES;
@@ -199,18 +225,18 @@ __global__ void __launch_bounds__(MX_THREADS, 1)
         const uint32_t t_im = t_re + (uint32_t)MX_BN;
         const int kb0 = set ? half : 0;
 #pragma unroll
-        for (int k8 = 0; k8 < MX_BK / 8; ++k8) {
+        for (int k8 = 0; k8 < MX_BK / 16; ++k8) {
           const uint32_t first = (kb != kb0 || k8) ? 1u : 0u;
 #pragma unroll
           for (int q = 0; q < 3; ++q)
-            umma_tf32(t_re, umma_desc_sw64(a_tile(s, ar_a[q]) + k8 * 32),
+            umma_f16(t_re, umma_desc_sw64(a_tile(s, ar_a[q]) + k8 * 32),
                       umma_desc_sw64(b_tile(s, ar_b[q]) + k8 * 32), id_wide,
                       (first | q) ? 1u : 0u);
 #pragma unroll
           for (int q = 0; q < 3; ++q) {
-            umma_tf32(t_re, umma_desc_sw64(a_tile(s, ai_a[q]) + k8 * 32),
+            umma_f16(t_re, umma_desc_sw64(a_tile(s, ai_a[q]) + k8 * 32),
                       umma_desc_sw64(b_tile(s, ai_bi[q]) + k8 * 32), id_neg, 1u);
-            umma_tf32(t_im, umma_desc_sw64(a_tile(s, ai_a[q]) + k8 * 32),
+            umma_f16(t_im, umma_desc_sw64(a_tile(s, ai_a[q]) + k8 * 32),
                       umma_desc_sw64(b_tile(s, ai_br[q]) + k8 * 32), id_pos, 1u);
           }
         }
@@ -231,6 +257,9 @@ __global__ void __launch_bounds__(MX_THREADS, 1)
     const bool use_beta = (p.beta.x != 0.0 || p.beta.y != 0.0);
     const double2* Cin = p.cin ? p.cin + (long long)b * p.sc : C;
     const cplx dg = mk(p.diag.x, p.diag.y);
+    const int* eB = p.eb + (long long)b * p.n;
+    // undo the power-of-two scaling of the operands: 2^-(row exponent of A)
+    const double row_unscale = row < p.m ? ldexp(1.0, -p.ea[(long long)b * p.m + row]) : 1.0;
     if (ok) {
       for (int c0 = 0; c0 < MX_BN; c0 += 16) {
         if (n0 + c0 >= p.n) break;  // warp-uniform
@@ -259,8 +288,9 @@ __global__ void __launch_bounds__(MX_THREADS, 1)
               // K halves: set 0 at columns [0, 2BN), set 1 (empty if nkb == 1) at [2BN, 4BN)
               const double s1r = nkb > 1 ? (double)__uint_as_float(cr[j]) : 0.0;
               const double s1i = nkb > 1 ? (double)__uint_as_float(ci[j]) : 0.0;
-              cplx v = alpha * mk((double)__uint_as_float(vr[j]) + s1r,
-                                  (double)__uint_as_float(vi[j]) + s1i);
+              const double f = row_unscale * ldexp(1.0, -eB[col]);
+              cplx v = alpha * mk(f * ((double)__uint_as_float(vr[j]) + s1r),
+                                  f * ((double)__uint_as_float(vi[j]) + s1i));
               if (use_beta) v = v + beta * mk(old[j].x, old[j].y);
               if (row == col) v = v + dg;
               C[row + (long long)col * p.ldc] = make_double2(v.x, v.y);
@@ -286,78 +316,151 @@ __global__ void __launch_bounds__(MX_THREADS, 1)
   }
 }
 
-// A (col-major complex M x K) -> planes [b][4][M][Kp], K contiguous (transpose
-// through a 32x32 shared tile).
+// x (FP64, already scaled by a power of two) -> x = hi + lo, hi = x rounded to
+// fp16, lo = the remainder rounded to fp16: hi*hi + hi*lo + lo*hi carries about
+// 22 significant bits of each product, as TF32x3 does.
+__device__ __forceinline__ void split_f16(double x, __half& hi, __half& lo) {
+  hi = __double2half(x);
+  lo = __double2half(x - (double)__half2float(hi));
+}
+
+// Exponent s with max |x| * 2^s in [2^14, 2^15): fp16 holds the scaled values
+// (largest finite 65504) with hi and lo normal down to 2^-14 of that range.
+__device__ __forceinline__ int scale_exponent(double mx) {
+  if (!(mx > 0.0) || !isfinite(mx)) return 0;
+  int e;
+  frexp(mx, &e);
+  return 15 - e;
+}
+
+// A (col-major complex M x K) -> planes [b][4][M][Kp] of fp16, K contiguous,
+// each row scaled by 2^ea[b][row] (the row's largest |re|, |im| to [2^14,
+// 2^15)).  One CTA per 32 rows: pass 1 finds the row maxima (lanes = rows, one
+// coalesced 512-byte column slice per warp load), pass 2 splits 32 x 32 tiles
+// transposed through shared memory (the slab is re-read from L2).
 __global__ void split_a_kernel(int M, int K, int Kp, const double2* A, long long lda,
-                               long long sa, float* out, const int* steps, int step) {
+                               long long sa, __half* out, int* ea, const int* steps, int step) {
   __shared__ double2 tile[32][33];
-  const int b = blockIdx.z;
+  __shared__ double red[8][32];
+  __shared__ double s_scale[32];
+  const int b = blockIdx.y;
   if (steps != nullptr && step >= steps[b]) return;  // inactive entry: the GEMM copies
-  const int m0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
+  const int m0 = blockIdx.x * 32;
   A += (long long)b * sa;
   const int tx = threadIdx.x, ty = threadIdx.y;
-  for (int j = ty; j < 32; j += 8) {
-    const int m = m0 + tx, k = k0 + j;
-    tile[j][tx] = (m < M && k < K) ? A[m + (long long)k * lda] : make_double2(0.0, 0.0);
+  {
+    double mx = 0.0;
+    const int r = m0 + tx;
+    if (r < M)
+      for (int k = ty; k < K; k += 8) {
+        const double2 v = A[r + (long long)k * lda];
+        mx = fmax(mx, fmax(fabs(v.x), fabs(v.y)));
+      }
+    red[ty][tx] = mx;
+  }
+  __syncthreads();
+  if (ty == 0) {
+    double mx = red[0][tx];
+    for (int j = 1; j < 8; ++j) mx = fmax(mx, red[j][tx]);
+    const int e = scale_exponent(mx);
+    s_scale[tx] = ldexp(1.0, e);
+    if (m0 + tx < M) ea[(long long)b * M + m0 + tx] = e;
   }
   __syncthreads();
   const long long plane = (long long)M * Kp;
-  float* o = out + (long long)b * MX_PLANES * plane;
-  for (int j = ty; j < 32; j += 8) {
-    const int m = m0 + j, k = k0 + tx;
-    if (m < M && k < Kp) {
-      const double2 v = tile[tx][j];
-      float rh, rl, ih, il;
-      split_tf32(v.x, rh, rl);
-      split_tf32(v.y, ih, il);
-      const long long off = (long long)m * Kp + k;
-      o[off] = rh;
-      o[plane + off] = rl;
-      o[2 * plane + off] = ih;
-      o[3 * plane + off] = il;
+  __half* o = out + (long long)b * MX_PLANES * plane;
+  for (int k0 = 0; k0 < Kp; k0 += 32) {
+    for (int j = ty; j < 32; j += 8) {
+      const int m = m0 + tx, k = k0 + j;
+      tile[j][tx] = (m < M && k < K) ? A[m + (long long)k * lda] : make_double2(0.0, 0.0);
     }
+    __syncthreads();
+    for (int j = ty; j < 32; j += 8) {
+      const int m = m0 + j, k = k0 + tx;
+      if (m < M && k < Kp) {
+        const double2 v = tile[tx][j];
+        const double sc = s_scale[j];
+        __half rh, rl, ih, il;
+        split_f16(v.x * sc, rh, rl);
+        split_f16(v.y * sc, ih, il);
+        const long long off = (long long)m * Kp + k;
+        o[off] = rh;
+        o[plane + off] = rl;
+        o[2 * plane + off] = ih;
+        o[3 * plane + off] = il;
+      }
+    }
+    __syncthreads();
   }
 }
 
-// B (col-major complex K x N) -> planes [b][4][N][Kp], K contiguous.
+// B (col-major complex K x N) -> planes [b][4][N][Kp] of fp16, K contiguous,
+// each column scaled by 2^eb[b][col]; one warp per column (max, then split).
 __global__ void split_b_kernel(int K, int N, int Kp, const double2* B, long long ldb,
-                               long long sb, float* out, const int* steps, int step) {
+                               long long sb, __half* out, int* eb, const int* steps, int step) {
   const int b = blockIdx.y;
   if (steps != nullptr && step >= steps[b]) return;
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (long long)N * Kp) return;
-  const int k = (int)(t % Kp), n = (int)(t / Kp);
-  B += (long long)b * sb;
-  const double2 v = k < K ? B[k + (long long)n * ldb] : make_double2(0.0, 0.0);
-  float rh, rl, ih, il;
-  split_tf32(v.x, rh, rl);
-  split_tf32(v.y, ih, il);
+  const int lane = threadIdx.x & 31;
+  const int n = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (n >= N) return;  // warp-uniform
+  const double2* col = B + (long long)b * sb + (long long)n * ldb;
+  double mx = 0.0;
+  for (int k = lane; k < K; k += 32) {
+    const double2 v = col[k];
+    mx = fmax(mx, fmax(fabs(v.x), fabs(v.y)));
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+  const int e = scale_exponent(mx);
+  if (lane == 0) eb[(long long)b * N + n] = e;
+  const double sc = ldexp(1.0, e);
   const long long plane = (long long)N * Kp;
-  float* o = out + (long long)b * MX_PLANES * plane;
-  o[t] = rh;
-  o[plane + t] = rl;
-  o[2 * plane + t] = ih;
-  o[3 * plane + t] = il;
+  __half* o = out + (long long)b * MX_PLANES * plane + (long long)n * Kp;
+  for (int k = lane; k < Kp; k += 32) {
+    const double2 v = k < K ? col[k] : make_double2(0.0, 0.0);
+    __half rh, rl, ih, il;
+    split_f16(v.x * sc, rh, rl);
+    split_f16(v.y * sc, ih, il);
+    o[k] = rh;
+    o[plane + k] = rl;
+    o[2 * plane + k] = ih;
+    o[3 * plane + k] = il;
+  }
 }
 
 // ------------------------------------------------------------------ host
-// planes tensor [batch*4][rows][kp] fp32 -> 3-D map (kp, rows, batch*4), box (16, box_rows, 1)
-static int make_map(CUtensorMap* map, float* base, int rows, int kp, int nplanes, int box_rows) {
+// planes tensor [batch*4][rows][kp] fp16 -> 3-D map (kp, rows, batch*4), box (32, box_rows, 1)
+static int make_map(CUtensorMap* map, __half* base, int rows, int kp, int nplanes, int box_rows) {
+  EncodeTiledFn enc = encode_fn();
+  if (!enc) {
+    euv_set_error("cuTensorMapEncodeTiled is not available from the driver");
+    return EUV_ERR_CUDA;
+  }
   const cuuint64_t dims[3] = {(cuuint64_t)kp, (cuuint64_t)rows, (cuuint64_t)nplanes};
-  const cuuint64_t strides[2] = {(cuuint64_t)kp * 4, (cuuint64_t)kp * 4 * rows};
+  const cuuint64_t strides[2] = {(cuuint64_t)kp * 2, (cuuint64_t)kp * 2 * rows};
   const cuuint32_t box[3] = {(cuuint32_t)MX_BK, (cuuint32_t)box_rows, 1};
-  return make_map_f32(map, base, 3, dims, strides, box);
+  const cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 3, base, dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    euv_set_error("cuTensorMapEncodeTiled failed (%d) for the fp16 planes", (int)r);
+    return EUV_ERR_CUDA;
+  }
+  return EUV_OK;
 }
 
 static inline int round_up(int x, int a) { return (x + a - 1) / a * a; }
 
 size_t gemm_mixed_workspace_bytes(int m, int n, int k, int batch) {
   const size_t kp = (size_t)round_up(k > 0 ? k : 1, MX_BK);
-  size_t a = (size_t)batch * MX_PLANES * (size_t)m * kp * 4;
-  size_t b = (size_t)batch * MX_PLANES * (size_t)n * kp * 4;
+  size_t a = (size_t)batch * MX_PLANES * (size_t)m * kp * 2;
+  size_t b = (size_t)batch * MX_PLANES * (size_t)n * kp * 2;
+  size_t e = (size_t)batch * (size_t)(m + n) * 4;
   a = (a + 1023) & ~(size_t)1023;
   b = (b + 1023) & ~(size_t)1023;
-  return a + b + 1024;
+  e = (e + 1023) & ~(size_t)1023;
+  return a + b + e + 1024;
 }
 
 int gemm_mixed(int m, int n, int k, cplx alpha, const double* scale, const double2* a,
@@ -378,27 +481,31 @@ int gemm_mixed(int m, int n, int k, cplx alpha, const double* scale, const doubl
     return EUV_ERR_WORKSPACE;
   }
   char* w = reinterpret_cast<char*>(work);
-  float* pa = reinterpret_cast<float*>(w);
-  size_t abytes = ((size_t)batch * MX_PLANES * (size_t)m * kp * 4 + 1023) & ~(size_t)1023;
-  float* pb = reinterpret_cast<float*>(w + abytes);
-  size_t bbytes = ((size_t)batch * MX_PLANES * (size_t)n * kp * 4 + 1023) & ~(size_t)1023;
+  __half* pa = reinterpret_cast<__half*>(w);
+  size_t abytes = ((size_t)batch * MX_PLANES * (size_t)m * kp * 2 + 1023) & ~(size_t)1023;
+  __half* pb = reinterpret_cast<__half*>(w + abytes);
+  size_t bbytes = ((size_t)batch * MX_PLANES * (size_t)n * kp * 2 + 1023) & ~(size_t)1023;
+  int* ea = reinterpret_cast<int*>(w + abytes + bbytes);
+  int* eb = ea + (size_t)batch * m;
+  size_t ebytes = ((size_t)batch * (size_t)(m + n) * 4 + 1023) & ~(size_t)1023;
   // the caller's sticky status word, else a per-call word in the workspace
   int* err = status;
   if (err == nullptr) {
-    err = reinterpret_cast<int*>(w + abytes + bbytes);
+    err = reinterpret_cast<int*>(w + abytes + bbytes + ebytes);
     EUV_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int), stream));
   }
-  // reuse bit 0 / bit 1: the A / B planes in this workspace are already those
-  // of the operand (the caller's previous call split the same unchanged
-  // matrix in the same role and shape), so the split is skipped
+  // reuse bit 0 / bit 1: the A / B planes (and scale exponents) in this
+  // workspace are already those of the operand (the caller's previous call
+  // split the same unchanged matrix in the same role and shape), so the split
+  // is skipped
   if (!(reuse & 1)) {
-    dim3 g((m + 31) / 32, (kp + 31) / 32, batch), t(32, 8);
-    split_a_kernel<<<g, t, 0, stream>>>(m, k, kp, a, lda, sa, pa, steps, step);
+    dim3 g((m + 31) / 32, batch), t(32, 8);
+    split_a_kernel<<<g, t, 0, stream>>>(m, k, kp, a, lda, sa, pa, ea, steps, step);
     EUV_LAUNCH_CHECK();
   }
   if (!(reuse & 2)) {
-    dim3 gb((unsigned)(((long long)n * kp + 255) / 256), batch);
-    split_b_kernel<<<gb, 256, 0, stream>>>(k, n, kp, b, ldb, sb, pb, steps, step);
+    dim3 gb((unsigned)((n + 7) / 8), batch);
+    split_b_kernel<<<gb, 256, 0, stream>>>(k, n, kp, b, ldb, sb, pb, eb, steps, step);
     EUV_LAUNCH_CHECK();
   }
   CUtensorMap ta, tb;
@@ -407,7 +514,7 @@ int gemm_mixed(int m, int n, int k, cplx alpha, const double* scale, const doubl
   rc = make_map(&tb, pb, n, kp, batch * MX_PLANES, MX_BN);
   if (rc) return rc;
   static int smem_done[64];
-  EUV_CUDA_TRY(ensure_smem(gemm_tf32x3_kernel, (int)MX_SMEM, smem_done));
+  EUV_CUDA_TRY(ensure_smem(gemm_split3_kernel, (int)MX_SMEM, smem_done));
   MixedArgs p;
   p.m = m;
   p.n = n;
@@ -426,8 +533,10 @@ int gemm_mixed(int m, int n, int k, cplx alpha, const double* scale, const doubl
   p.steps = steps;
   p.step = step;
   p.err = err;
+  p.ea = ea;
+  p.eb = eb;
   dim3 grid((m + MX_BM - 1) / MX_BM, (n + MX_BN - 1) / MX_BN, batch);
-  gemm_tf32x3_kernel<<<grid, MX_THREADS, MX_SMEM, stream>>>(ta, tb, p);
+  gemm_split3_kernel<<<grid, MX_THREADS, MX_SMEM, stream>>>(ta, tb, p);
   EUV_LAUNCH_CHECK();
   return EUV_OK;
 }
@@ -436,12 +545,12 @@ int gemm_mixed(int m, int n, int k, cplx alpha, const double* scale, const doubl
 
 using namespace euv;
 
-extern "C" size_t euv_zgemm_tf32x3_workspace_bytes(int m, int n, int k, int batch) {
+extern "C" size_t euv_zgemm_mixed_workspace_bytes(int m, int n, int k, int batch) {
   if (m <= 0 || n <= 0 || k <= 0 || batch <= 0) return 0;
   return gemm_mixed_workspace_bytes(m, n, k, batch);
 }
 
-extern "C" int euv_zgemm_tf32x3(int m, int n, int k, euv_c64 alpha, const double* d_scale,
+extern "C" int euv_zgemm_mixed(int m, int n, int k, euv_c64 alpha, const double* d_scale,
                                 const euv_c64* d_a, int lda, long long stride_a,
                                 const euv_c64* d_b, int ldb, long long stride_b, euv_c64 beta,
                                 euv_c64* d_c, int ldc, long long stride_c, euv_c64 diag,
@@ -449,7 +558,7 @@ extern "C" int euv_zgemm_tf32x3(int m, int n, int k, euv_c64 alpha, const double
                                 size_t work_bytes, int* d_status, void* stream) {
   if (m <= 0 || n <= 0 || k <= 0 || batch <= 0 || lda < m || ldc < m || ldb < k || !d_a ||
       !d_b || !d_c || (d_steps != nullptr && (m != n || m != k))) {
-    euv_set_error("euv_zgemm_tf32x3: bad arguments (m=%d n=%d k=%d)", m, n, k);
+    euv_set_error("euv_zgemm_mixed: bad arguments (m=%d n=%d k=%d)", m, n, k);
     return EUV_ERR_BAD_ARG;
   }
   return gemm_mixed(m, n, k, fromc(alpha), d_scale, reinterpret_cast<const double2*>(d_a), lda,

@@ -43,7 +43,7 @@ size_t gemm_mixed_workspace_bytes(int m, int n, int k, int batch);
 
 // ||A||_1 bound for the degree-8 Taylor step of cos/sin(sqrt(A)): the dropped
 // term is ~theta^9/18!, 1.6e-16 at theta = 1 (FP64) and 2e-8 at theta = 8,
-// which the mixed form uses (its TF32x3 products carry ~1e-6 relative error,
+// which the mixed form uses (its split-FP16x3 products carry ~1e-6 relative error,
 // and each double-angle step saved also saves its error growth).
 constexpr double kThetaFp64 = 1.0;
 constexpr double kThetaMixed = 8.0;
@@ -550,7 +550,7 @@ __global__ void flag_singular_kernel(const int* info, int n, int* status) {
   if (i < n && info[i] != 0) atomicOr(status, EUV_STATUS_SINGULAR);
 }
 
-// GEMM dispatch by precision (FP64 DMMA, or TF32x3 tcgen05 tensor cores for
+// GEMM dispatch by precision (FP64 DMMA, or split-FP16x3 tcgen05 tensor cores for
 // the bulk products of the mixed form; `status` receives EUV_STATUS_TIMEOUT).
 // Gemm reuse flags (mixed form only): the previous call through the same Gemm
 // split this unchanged operand in the same role and shape, so its TF32 planes
@@ -695,7 +695,7 @@ static int euler_factors(const euv_amp_desc* d) {
   }
   const double e = (kp / d->k) * (kp / d->k) * sup;
   if (!(e < 0.5)) return 0;
-  // The product serves the mixed form only, whose TF32x3 products carry ~1e-6
+  // The product serves the mixed form only, whose split-FP16x3 products carry ~1e-6
   // relative error each: a truncation ||E||^(2^F) <= 1e-7 stays below that.
   // the product of F factors is sum_{j < 2^F} E^j: truncation ||E||^(2^F)
   int f = 1;
@@ -1028,7 +1028,7 @@ extern "C" int euv_amp(const euv_amp_desc* d, const euv_c64* d_spectra, euv_c64*
     EUV_LAUNCH_CHECK();
     if ((rc = lu_solve(N, ns, w.G, N, nn, w.ipiv, w.E, N, (long long)N * ns, U, stream))) return rc;
     // Y Z for the source columns: a product, so the mixed form takes it on the
-    // tensor cores (TF32x3, ~1e-6 relative) like the matrix functions; the
+    // tensor cores (split-FP16x3, ~1e-6 relative) like the matrix functions; the
     // solve above stays FP64
     if ((rc = gemm(N, ns, N, one, nullptr, Y, N, nn, w.E, N, (long long)N * ns, zero, w.YZ, N,
                    (long long)N * ns, zero, U)))

@@ -1,6 +1,6 @@
 """Kernel microbenchmarks at the shapes of the measured workloads.
 
-  python -m euvlitho_b200.microbench tf32x3 --n 961 --batch 4
+  python -m euvlitho_b200.microbench mixed  --n 961 --batch 4
   python -m euvlitho_b200.microbench zgemm  --n 961 --batch 4
   python -m euvlitho_b200.microbench lu     --n 961 --batch 24 --nrhs 96
   python -m euvlitho_b200.microbench step   --precision mixed --clips 4
@@ -243,7 +243,7 @@ def _time(fn, reps: int) -> float:
 
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("kernel", choices=["tf32x3", "zgemm", "lu", "step", "linear", "raster",
+    ap.add_argument("kernel", choices=["mixed", "zgemm", "lu", "step", "linear", "raster",
                                        "socs", "cnn", "summarize"])
     ap.add_argument("--slices", type=int, default=8)
     ap.add_argument("csv", nargs="?", help="ncu --csv launch list (summarize)")
@@ -281,15 +281,15 @@ def main(argv=None) -> int:
     g = torch.Generator(device="cuda").manual_seed(0)
     A = torch.randn(b, n, n, dtype=torch.complex128, device="cuda", generator=g)
     out = {"kernel": a.kernel, "n": n, "batch": b}
-    if a.kernel in ("tf32x3", "zgemm"):
+    if a.kernel in ("mixed", "zgemm"):
         B = torch.randn(b, n, n, dtype=torch.complex128, device="cuda", generator=g)
         C = torch.empty_like(A)
-        if a.kernel == "tf32x3":
-            wb = L.lib().euv_zgemm_tf32x3_workspace_bytes(n, n, n, b)
+        if a.kernel == "mixed":
+            wb = L.lib().euv_zgemm_mixed_workspace_bytes(n, n, n, b)
             ws = torch.empty(wb, dtype=torch.uint8, device="cuda")
 
             def fn():
-                L.call("euv_zgemm_tf32x3", n, n, n, L.c64(1, 0), None, A.data_ptr(), n, n * n,
+                L.call("euv_zgemm_mixed", n, n, n, L.c64(1, 0), None, A.data_ptr(), n, n * n,
                        B.data_ptr(), n, n * n, L.c64(0, 0), C.data_ptr(), n, n * n, L.c64(0, 0),
                        b, None, 0, ws.data_ptr(), wb, None, s)
         else:

@@ -42,7 +42,7 @@ extern "C" {
 #define EUV_ERR_TIMEOUT 5  /* a bounded device wait expired (euv_wait_probe) */
 
 /* Bits of a caller-owned device status word (euv_amp_desc.d_status, the d_status
- * argument of euv_zgemm_tf32x3 and euv_wait_probe).  The library only ORs bits
+ * argument of euv_zgemm_mixed and euv_wait_probe).  The library only ORs bits
  * in; the caller zeroes the word and reads it when the stream is idle (the
  * reference checks none of these conditions, header.h:498,888,1529). */
 #define EUV_STATUS_TIMEOUT 1       /* a bounded device wait gave up: that call's results are incomplete */
@@ -53,7 +53,7 @@ extern "C" {
 #define EUV_MAX_SLICES 32
 
 #define EUV_PREC_FP64 0  /* every product in FP64 */
-#define EUV_PREC_MIXED 1 /* bulk products as TF32x3 on tcgen05 tensor cores, FP64 solves */
+#define EUV_PREC_MIXED 1 /* bulk products as split-FP16x3 on tcgen05 tensor cores, FP64 solves */
 
 typedef struct {
   double re, im;
@@ -515,13 +515,15 @@ int euv_zgemm(int m, int n, int k, euv_c64 alpha, const double* d_scale, const e
               int batch, const int* d_steps, int step, void* stream);
 
 /* The bulk product of EUV_PREC_MIXED: same contract as euv_zgemm, computed on
- * the tcgen05 tensor cores as TF32x3 (each FP64 operand split into two TF32
- * terms, three TF32 products per real product, FP32 accumulation; ~1e-6
- * relative error per product).  Needs a workspace for the split operands.
- * d_status (optional device int): EUV_STATUS_TIMEOUT is OR-ed in if one of the
- * kernel's bounded waits (about 2 s) gave up. */
-size_t euv_zgemm_tf32x3_workspace_bytes(int m, int n, int k, int batch);
-int euv_zgemm_tf32x3(int m, int n, int k, euv_c64 alpha, const double* d_scale,
+ * the tcgen05 tensor cores as split-FP16x3: each row of A and column of B is
+ * scaled by a power of two into fp16's range, each scaled FP64 value split
+ * into two fp16 terms, three fp16 products per real product (kind::f16, FP32
+ * accumulation), the scaling undone in FP64 (~1e-6 relative error per product,
+ * about that of TF32x3 at twice its tensor rate).  Needs a workspace for the
+ * split operands.  d_status (optional device int): EUV_STATUS_TIMEOUT is
+ * OR-ed in if one of the kernel's bounded waits (about 2 s) gave up. */
+size_t euv_zgemm_mixed_workspace_bytes(int m, int n, int k, int batch);
+int euv_zgemm_mixed(int m, int n, int k, euv_c64 alpha, const double* d_scale,
                      const euv_c64* d_a, int lda, long long stride_a, const euv_c64* d_b, int ldb,
                      long long stride_b, euv_c64 beta, euv_c64* d_c, int ldc, long long stride_c,
                      euv_c64 diag, int batch, const int* d_steps, int step, void* d_work,

@@ -179,8 +179,8 @@ def test_mask_spectrum_batch(cuda):
 
 @pytest.mark.parametrize("m,n,k,batch", [(128, 256, 16, 1), (121, 121, 121, 2), (300, 200, 77, 2), (961, 961, 961, 2),
                                          (130, 144, 50, 1), (70, 16, 33, 1), (65, 130, 40, 3)])
-def test_zgemm_tf32x3(cuda, m, n, k, batch):
-    """tcgen05 TF32x3 complex GEMM against NumPy FP64.  The bound is set by the
+def test_zgemm_mixed(cuda, m, n, k, batch):
+    """tcgen05 split-FP16x3 complex GEMM against NumPy FP64.  The bound is set by the
     FP32 accumulation in tensor memory (grows with K: ~1.5e-5 at K = 961)."""
     import torch
     rng = np.random.default_rng(7 * m + n + k)
@@ -189,10 +189,10 @@ def test_zgemm_tf32x3(cuda, m, n, k, batch):
     Cm = rng.standard_normal((batch, m, n)) + 1j * rng.standard_normal((batch, m, n))
     alpha, beta, diag = 0.5 + 0.25j, 0.3 - 0.1j, -1.0 + 0.0j
     dA, dB, dC = _t(_colmajor(A), cuda), _t(_colmajor(B), cuda), _t(_colmajor(Cm), cuda)
-    wb = L.lib().euv_zgemm_tf32x3_workspace_bytes(m, n, k, batch)
+    wb = L.lib().euv_zgemm_mixed_workspace_bytes(m, n, k, batch)
     ws = torch.empty(wb, dtype=torch.uint8, device=cuda)
     st = torch.zeros(1, dtype=torch.int32, device=cuda)
-    L.call("euv_zgemm_tf32x3", m, n, k, L.c64.of(alpha), None, dA.data_ptr(), m, m * k,
+    L.call("euv_zgemm_mixed", m, n, k, L.c64.of(alpha), None, dA.data_ptr(), m, m * k,
            dB.data_ptr(), k, k * n, L.c64.of(beta), dC.data_ptr(), m, m * n, L.c64.of(diag), batch,
            None, 0, ws.data_ptr(), wb, st.data_ptr(), _stream())
     torch.cuda.synchronize()
@@ -204,7 +204,7 @@ def test_zgemm_tf32x3(cuda, m, n, k, batch):
     assert rel_err(got, ref) < 3e-8 * k + 1e-6
 
 
-def test_zgemm_tf32x3_step_copy(cuda):
+def test_zgemm_mixed_step_copy(cuda):
     import torch
     n, batch = 130, 2
     rng = np.random.default_rng(1)
@@ -212,9 +212,9 @@ def test_zgemm_tf32x3_step_copy(cuda):
     dA = _t(_colmajor(A), cuda)
     dC = torch.zeros_like(dA)
     steps = _t(np.array([0, 3], np.int32), cuda)
-    wb = L.lib().euv_zgemm_tf32x3_workspace_bytes(n, n, n, batch)
+    wb = L.lib().euv_zgemm_mixed_workspace_bytes(n, n, n, batch)
     ws = torch.empty(wb, dtype=torch.uint8, device=cuda)
-    L.call("euv_zgemm_tf32x3", n, n, n, L.c64.of(1.0), None, dA.data_ptr(), n, n * n,
+    L.call("euv_zgemm_mixed", n, n, n, L.c64.of(1.0), None, dA.data_ptr(), n, n * n,
            dA.data_ptr(), n, n * n, L.c64.of(0), dC.data_ptr(), n, n * n, L.c64.of(0), batch,
            steps.data_ptr(), 1, ws.data_ptr(), wb, None, _stream())
     torch.cuda.synchronize()
@@ -241,7 +241,7 @@ def test_matfun_mixed_close_to_fp64(cuda):
                prec, ws.data_ptr(), wb, _stream())
         torch.cuda.synchronize()
         out[prec] = (dc.cpu().numpy(), ds.cpu().numpy())
-    # ~5e-6 per TF32x3 product, amplified by the ~6 double-angle steps of a
+    # ~5e-6 per split-FP16x3 product, amplified by the ~6 double-angle steps of a
     # 60 nm slice; the end-to-end bar (intensity < 1e-4) is in test_gpu_parity
     assert rel_err(out[L.EUV_PREC_MIXED][0], out[L.EUV_PREC_FP64][0]) < 1e-3
     assert rel_err(out[L.EUV_PREC_MIXED][1], out[L.EUV_PREC_FP64][1]) < 1e-3

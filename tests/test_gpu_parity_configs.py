@@ -15,7 +15,7 @@ Bars (max |x - x_ref| / max |x_ref| per output array): the FP64 form 1e-8
 two algorithms).  The mixed form: images 1e-4 (the north-star intensity bar);
 amplitudes 5e-4 and M3D parameters 1e-3 of max |a0|, the measured envelopes
 with about 2x margin (B200: amplitudes up to 2.6e-4 for a 60 nm single slab
-with 41x41 orders, where the double-angle steps amplify the TF32x3 product
+with 41x41 orders, where the double-angle steps amplify the split-FP16x3 product
 errors; the M3D intercept a0 5.3e-4 at 31x31 orders, since the fit works on
 the small difference between rigorous and thin-mask amplitudes).  The images
 sum |E|^2 over hundreds of source points and stay within 6e-5.  M3D slopes
