@@ -215,32 +215,45 @@ __global__ void __launch_bounds__(MX_THREADS, 1)
       const uint32_t id_pos = idesc_f16(false), id_neg = idesc_f16(true);
       const uint32_t id_wide = idesc_f16_mn(false, MX_BM, 2 * MX_BN);
       const int half = (nkb + 1) / 2;  // k-blocks [0, half) -> set 0, [half, nkb) -> set 1
+      // Shared-memory descriptors of stage 0, computed once: the tile of stage s
+      // lies s * MX_STAGE_BYTES further and a K16 step 32 bytes further, i.e.
+      // + s * (MX_STAGE_BYTES >> 4) and + 2 in the 14-bit address field, which
+      // cannot carry (shared addresses stay below 2^18).  The issue loop then
+      // only adds.
+      uint64_t dA[MX_PLANES], dB[MX_PLANES];
+#pragma unroll
+      for (int pl = 0; pl < MX_PLANES; ++pl) {
+        dA[pl] = umma_desc_sw64(a_tile(0, pl));
+        dB[pl] = umma_desc_sw64(b_tile(0, pl));
+      }
+      int s = 0;
+      uint32_t ph = 0;
       for (int kb = 0; kb < nkb; ++kb) {
-        const int s = kb % MX_STAGES;
-        const uint32_t ph = (uint32_t)((kb / MX_STAGES) & 1);
         if (!mbar_wait(&full[s], ph, abort_flag, p.err)) break;
         tc_fence_after();
         const int set = kb < half ? 0 : 1;
         const uint32_t t_re = tmem + (uint32_t)(2 * set * MX_BN);
         const uint32_t t_im = t_re + (uint32_t)MX_BN;
         const int kb0 = set ? half : 0;
+        const uint64_t so = (uint64_t)s * (uint64_t)(MX_STAGE_BYTES >> 4);
 #pragma unroll
-        for (int k8 = 0; k8 < MX_BK / 16; ++k8) {
-          const uint32_t first = (kb != kb0 || k8) ? 1u : 0u;
+        for (int k16 = 0; k16 < MX_BK / 16; ++k16) {
+          const uint32_t first = (kb != kb0 || k16) ? 1u : 0u;
+          const uint64_t ko = so + (uint64_t)(2 * k16);
 #pragma unroll
           for (int q = 0; q < 3; ++q)
-            umma_f16(t_re, umma_desc_sw64(a_tile(s, ar_a[q]) + k8 * 32),
-                      umma_desc_sw64(b_tile(s, ar_b[q]) + k8 * 32), id_wide,
-                      (first | q) ? 1u : 0u);
+            umma_f16(t_re, dA[ar_a[q]] + ko, dB[ar_b[q]] + ko, id_wide, (first | q) ? 1u : 0u);
 #pragma unroll
           for (int q = 0; q < 3; ++q) {
-            umma_f16(t_re, umma_desc_sw64(a_tile(s, ai_a[q]) + k8 * 32),
-                      umma_desc_sw64(b_tile(s, ai_bi[q]) + k8 * 32), id_neg, 1u);
-            umma_f16(t_im, umma_desc_sw64(a_tile(s, ai_a[q]) + k8 * 32),
-                      umma_desc_sw64(b_tile(s, ai_br[q]) + k8 * 32), id_pos, 1u);
+            umma_f16(t_re, dA[ai_a[q]] + ko, dB[ai_bi[q]] + ko, id_neg, 1u);
+            umma_f16(t_im, dA[ai_a[q]] + ko, dB[ai_br[q]] + ko, id_pos, 1u);
           }
         }
         umma_commit(&empty[s]);  // frees the stage when these MMAs complete
+        if (++s == MX_STAGES) {
+          s = 0;
+          ph ^= 1u;
+        }
       }
       umma_commit(accum);  // always: the epilogue / teardown waits on it
     }
@@ -428,6 +441,188 @@ __global__ void split_b_kernel(int K, int N, int Kp, const double2* B, long long
   }
 }
 
+// The same splits with the operand's slab staged in shared memory, so that HBM
+// sees one read and the plane writes (the two-pass kernels above re-read the
+// slab, from HBM once the slabs of all resident CTAs exceed L2).  R rows of A
+// (or R columns of B) per CTA, R * K * 16 bytes of shared memory; used when
+// that fits (split_slab_rows), the two-pass kernels otherwise.
+constexpr size_t MX_SLAB_BYTES = 100 * 1024;      // several CTAs per SM
+constexpr size_t MX_SLAB_BYTES_ONE = 200 * 1024;  // one row or column per CTA
+constexpr int MX_SLAB_THREADS = 256;
+constexpr int MX_SLAB_UNROLL = 8;
+
+template <int R>
+__global__ void __launch_bounds__(MX_SLAB_THREADS)
+    split_a_slab_kernel(int M, int K, int Kp, const double2* A, long long lda, long long sa,
+                        __half* out, int* ea, const int* steps, int step) {
+  extern __shared__ double2 slab[];  // [K][R]: element (row r, column k) at k * R + r
+  __shared__ double s_scale[R];
+  const int b = blockIdx.y;
+  if (steps != nullptr && step >= steps[b]) return;  // inactive entry: the GEMM copies
+  const int m0 = blockIdx.x * R;
+  const int rows = M - m0 < R ? M - m0 : R;
+  A += (long long)b * sa;
+  // consecutive threads take consecutive rows of a column (runs of R * 16
+  // bytes); eight loads in flight per thread before their stores
+  for (int base = 0; base < K * R; base += MX_SLAB_THREADS * MX_SLAB_UNROLL) {
+    double2 v[MX_SLAB_UNROLL];
+#pragma unroll
+    for (int u = 0; u < MX_SLAB_UNROLL; ++u) {
+      const int t = base + threadIdx.x + u * MX_SLAB_THREADS;
+      const int k = t / R, r = t % R;
+      v[u] = (t < K * R && r < rows) ? A[(m0 + r) + (long long)k * lda] : make_double2(0.0, 0.0);
+    }
+#pragma unroll
+    for (int u = 0; u < MX_SLAB_UNROLL; ++u) {
+      const int t = base + threadIdx.x + u * MX_SLAB_THREADS;
+      if (t < K * R) slab[t] = v[u];
+    }
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (warp < R) {
+    double mx = 0.0;
+    for (int k = lane; k < K; k += 32) {
+      const double2 v = slab[k * R + warp];
+      mx = fmax(mx, fmax(fabs(v.x), fabs(v.y)));
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+    if (lane == 0) {
+      const int e = scale_exponent(mx);
+      s_scale[warp] = ldexp(1.0, e);
+      if (warp < rows) ea[(long long)b * M + m0 + warp] = e;
+    }
+  }
+  __syncthreads();
+  const long long plane = (long long)M * Kp;
+  __half* o = out + (long long)b * MX_PLANES * plane;
+  for (int t = threadIdx.x; t < rows * Kp; t += MX_SLAB_THREADS) {
+    const int r = t / Kp, k = t % Kp;
+    const double2 v = k < K ? slab[k * R + r] : make_double2(0.0, 0.0);
+    const double sc = s_scale[r];
+    __half rh, rl, ih, il;
+    split_f16(v.x * sc, rh, rl);
+    split_f16(v.y * sc, ih, il);
+    const long long off = (long long)(m0 + r) * Kp + k;
+    o[off] = rh;
+    o[plane + off] = rl;
+    o[2 * plane + off] = ih;
+    o[3 * plane + off] = il;
+  }
+}
+
+template <int R>
+__global__ void __launch_bounds__(MX_SLAB_THREADS)
+    split_b_slab_kernel(int K, int N, int Kp, const double2* B, long long ldb, long long sb,
+                        __half* out, int* eb, const int* steps, int step) {
+  extern __shared__ double2 slab[];  // [R][K]: element (k, column c) at c * K + k
+  __shared__ double s_scale[R];
+  const int b = blockIdx.y;
+  if (steps != nullptr && step >= steps[b]) return;
+  const int n0 = blockIdx.x * R;
+  const int cols = N - n0 < R ? N - n0 : R;
+  B += (long long)b * sb;
+  for (int base = 0; base < K * R; base += MX_SLAB_THREADS * MX_SLAB_UNROLL) {
+    double2 v[MX_SLAB_UNROLL];
+#pragma unroll
+    for (int u = 0; u < MX_SLAB_UNROLL; ++u) {
+      const int t = base + threadIdx.x + u * MX_SLAB_THREADS;
+      const int c = t / K, k = t % K;
+      v[u] = (t < K * R && c < cols) ? B[k + (long long)(n0 + c) * ldb] : make_double2(0.0, 0.0);
+    }
+#pragma unroll
+    for (int u = 0; u < MX_SLAB_UNROLL; ++u) {
+      const int t = base + threadIdx.x + u * MX_SLAB_THREADS;
+      if (t < K * R) slab[t] = v[u];
+    }
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (warp < R) {
+    double mx = 0.0;
+    for (int k = lane; k < K; k += 32) {
+      const double2 v = slab[warp * K + k];
+      mx = fmax(mx, fmax(fabs(v.x), fabs(v.y)));
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+    if (lane == 0) {
+      const int e = scale_exponent(mx);
+      s_scale[warp] = ldexp(1.0, e);
+      if (warp < cols) eb[(long long)b * N + n0 + warp] = e;
+    }
+  }
+  __syncthreads();
+  const long long plane = (long long)N * Kp;
+  __half* o = out + (long long)b * MX_PLANES * plane;
+  for (int t = threadIdx.x; t < cols * Kp; t += MX_SLAB_THREADS) {
+    const int c = t / Kp, k = t % Kp;
+    const double2 v = k < K ? slab[c * K + k] : make_double2(0.0, 0.0);
+    const double sc = s_scale[c];
+    __half rh, rl, ih, il;
+    split_f16(v.x * sc, rh, rl);
+    split_f16(v.y * sc, ih, il);
+    const long long off = (long long)(n0 + c) * Kp + k;
+    o[off] = rh;
+    o[plane + off] = rl;
+    o[2 * plane + off] = ih;
+    o[3 * plane + off] = il;
+  }
+}
+
+// Rows (columns) per CTA of the slab splits: the most of 8, 4, 2 whose slab
+// fits MX_SLAB_BYTES (so that several CTAs share an SM and keep enough loads
+// in flight), else 1 up to MX_SLAB_BYTES_ONE; 0 beyond (the two-pass kernels).
+static int split_slab_rows(int K) {
+  const size_t row = (size_t)K * sizeof(double2);
+  for (int r = 8; r >= 2; r >>= 1)
+    if ((size_t)r * row <= MX_SLAB_BYTES) return r;
+  return row <= MX_SLAB_BYTES_ONE ? 1 : 0;
+}
+
+template <int R>
+static int launch_split_slab(bool a_role, int rows, int K, int Kp, const double2* X, long long ld,
+                             long long st, __half* out, int* ex, int batch, const int* steps,
+                             int step, cudaStream_t stream) {
+  static int done_a[64], done_b[64];
+  const int smem = R * K * (int)sizeof(double2);
+  dim3 g((unsigned)((rows + R - 1) / R), batch);
+  if (a_role) {
+    EUV_CUDA_TRY(ensure_smem(split_a_slab_kernel<R>, smem, done_a));
+    split_a_slab_kernel<R><<<g, MX_SLAB_THREADS, smem, stream>>>(rows, K, Kp, X, ld, st, out, ex,
+                                                                  steps, step);
+  } else {
+    EUV_CUDA_TRY(ensure_smem(split_b_slab_kernel<R>, smem, done_b));
+    split_b_slab_kernel<R><<<g, MX_SLAB_THREADS, smem, stream>>>(K, rows, Kp, X, ld, st, out, ex,
+                                                                  steps, step);
+  }
+  EUV_LAUNCH_CHECK();
+  return EUV_OK;
+}
+
+// Split of one operand: A role (rows = M) or B role (rows = N, the columns).
+static int split_operand(bool a_role, int rows, int K, int Kp, const double2* X, long long ld,
+                         long long st, __half* out, int* ex, int batch, const int* steps, int step,
+                         cudaStream_t stream) {
+  switch (split_slab_rows(K)) {
+    case 8: return launch_split_slab<8>(a_role, rows, K, Kp, X, ld, st, out, ex, batch, steps, step, stream);
+    case 4: return launch_split_slab<4>(a_role, rows, K, Kp, X, ld, st, out, ex, batch, steps, step, stream);
+    case 2: return launch_split_slab<2>(a_role, rows, K, Kp, X, ld, st, out, ex, batch, steps, step, stream);
+    case 1: return launch_split_slab<1>(a_role, rows, K, Kp, X, ld, st, out, ex, batch, steps, step, stream);
+    default: break;
+  }
+  if (a_role) {
+    dim3 g((rows + 31) / 32, batch), t(32, 8);
+    split_a_kernel<<<g, t, 0, stream>>>(rows, K, Kp, X, ld, st, out, ex, steps, step);
+  } else {
+    dim3 gb((unsigned)((rows + 7) / 8), batch);
+    split_b_kernel<<<gb, 256, 0, stream>>>(K, rows, Kp, X, ld, st, out, ex, steps, step);
+  }
+  EUV_LAUNCH_CHECK();
+  return EUV_OK;
+}
+
 // ------------------------------------------------------------------ host
 // planes tensor [batch*4][rows][kp] fp16 -> 3-D map (kp, rows, batch*4), box (32, box_rows, 1)
 static int make_map(CUtensorMap* map, __half* base, int rows, int kp, int nplanes, int box_rows) {
@@ -498,18 +693,15 @@ int gemm_mixed(int m, int n, int k, cplx alpha, const double* scale, const doubl
   // workspace are already those of the operand (the caller's previous call
   // split the same unchanged matrix in the same role and shape), so the split
   // is skipped
-  if (!(reuse & 1)) {
-    dim3 g((m + 31) / 32, batch), t(32, 8);
-    split_a_kernel<<<g, t, 0, stream>>>(m, k, kp, a, lda, sa, pa, ea, steps, step);
-    EUV_LAUNCH_CHECK();
-  }
-  if (!(reuse & 2)) {
-    dim3 gb((unsigned)((n + 7) / 8), batch);
-    split_b_kernel<<<gb, 256, 0, stream>>>(k, n, kp, b, ldb, sb, pb, eb, steps, step);
-    EUV_LAUNCH_CHECK();
-  }
+  int rc;
+  if (!(reuse & 1) &&
+      (rc = split_operand(true, m, k, kp, a, lda, sa, pa, ea, batch, steps, step, stream)))
+    return rc;
+  if (!(reuse & 2) &&
+      (rc = split_operand(false, n, k, kp, b, ldb, sb, pb, eb, batch, steps, step, stream)))
+    return rc;
   CUtensorMap ta, tb;
-  int rc = make_map(&ta, pa, m, kp, batch * MX_PLANES, MX_BM);
+  rc = make_map(&ta, pa, m, kp, batch * MX_PLANES, MX_BM);
   if (rc) return rc;
   rc = make_map(&tb, pb, n, kp, batch * MX_PLANES, MX_BN);
   if (rc) return rc;
