@@ -451,11 +451,20 @@ constexpr size_t MX_SLAB_BYTES_ONE = 200 * 1024;  // one row or column per CTA
 constexpr int MX_SLAB_THREADS = 256;
 constexpr int MX_SLAB_UNROLL = 8;
 
+// Row stride (elements) of the A slab: K rounded up to 8, plus 8 / R, so that
+// the loads' stores (R consecutive rows per run of lanes) and the row-wise
+// reads of the split both hit distinct 16-byte bank groups.
+template <int R>
+__host__ __device__ constexpr int slab_a_stride(int K) {
+  return ((K + 7) / 8) * 8 + (R > 1 ? 8 / R : 0);
+}
+
 template <int R>
 __global__ void __launch_bounds__(MX_SLAB_THREADS)
     split_a_slab_kernel(int M, int K, int Kp, const double2* A, long long lda, long long sa,
                         __half* out, int* ea, const int* steps, int step) {
-  extern __shared__ double2 slab[];  // [K][R]: element (row r, column k) at k * R + r
+  extern __shared__ double2 slab[];  // [R][Ks]: element (row r, column k) at r * Ks + k
+  const int Ks = slab_a_stride<R>(K);
   __shared__ double s_scale[R];
   const int b = blockIdx.y;
   if (steps != nullptr && step >= steps[b]) return;  // inactive entry: the GEMM copies
@@ -475,7 +484,7 @@ __global__ void __launch_bounds__(MX_SLAB_THREADS)
 #pragma unroll
     for (int u = 0; u < MX_SLAB_UNROLL; ++u) {
       const int t = base + threadIdx.x + u * MX_SLAB_THREADS;
-      if (t < K * R) slab[t] = v[u];
+      if (t < K * R) slab[(t % R) * Ks + t / R] = v[u];
     }
   }
   __syncthreads();
@@ -483,7 +492,7 @@ __global__ void __launch_bounds__(MX_SLAB_THREADS)
   if (warp < R) {
     double mx = 0.0;
     for (int k = lane; k < K; k += 32) {
-      const double2 v = slab[k * R + warp];
+      const double2 v = slab[warp * Ks + k];
       mx = fmax(mx, fmax(fabs(v.x), fabs(v.y)));
     }
 #pragma unroll
@@ -497,18 +506,24 @@ __global__ void __launch_bounds__(MX_SLAB_THREADS)
   __syncthreads();
   const long long plane = (long long)M * Kp;
   __half* o = out + (long long)b * MX_PLANES * plane;
-  for (int t = threadIdx.x; t < rows * Kp; t += MX_SLAB_THREADS) {
-    const int r = t / Kp, k = t % Kp;
-    const double2 v = k < K ? slab[k * R + r] : make_double2(0.0, 0.0);
+  // two consecutive k per thread: one 4-byte store per plane (Kp is even)
+  const int kh = Kp >> 1;
+  for (int t = threadIdx.x; t < rows * kh; t += MX_SLAB_THREADS) {
+    const int r = t / kh, k = 2 * (t % kh);
+    const double2 v0 = k < K ? slab[r * Ks + k] : make_double2(0.0, 0.0);
+    const double2 v1 = k + 1 < K ? slab[r * Ks + k + 1] : make_double2(0.0, 0.0);
     const double sc = s_scale[r];
-    __half rh, rl, ih, il;
-    split_f16(v.x * sc, rh, rl);
-    split_f16(v.y * sc, ih, il);
-    const long long off = (long long)(m0 + r) * Kp + k;
-    o[off] = rh;
-    o[plane + off] = rl;
-    o[2 * plane + off] = ih;
-    o[3 * plane + off] = il;
+    __half2 rh, rl, ih, il;
+    split_f16(v0.x * sc, rh.x, rl.x);
+    split_f16(v0.y * sc, ih.x, il.x);
+    split_f16(v1.x * sc, rh.y, rl.y);
+    split_f16(v1.y * sc, ih.y, il.y);
+    __half2* o2 = reinterpret_cast<__half2*>(o + (long long)(m0 + r) * Kp + k);
+    const long long p2 = plane >> 1;
+    o2[0] = rh;
+    o2[p2] = rl;
+    o2[2 * p2] = ih;
+    o2[3 * p2] = il;
   }
 }
 
@@ -556,18 +571,23 @@ __global__ void __launch_bounds__(MX_SLAB_THREADS)
   __syncthreads();
   const long long plane = (long long)N * Kp;
   __half* o = out + (long long)b * MX_PLANES * plane;
-  for (int t = threadIdx.x; t < cols * Kp; t += MX_SLAB_THREADS) {
-    const int c = t / Kp, k = t % Kp;
-    const double2 v = k < K ? slab[c * K + k] : make_double2(0.0, 0.0);
+  const int kh = Kp >> 1;
+  for (int t = threadIdx.x; t < cols * kh; t += MX_SLAB_THREADS) {
+    const int c = t / kh, k = 2 * (t % kh);
+    const double2 v0 = k < K ? slab[c * K + k] : make_double2(0.0, 0.0);
+    const double2 v1 = k + 1 < K ? slab[c * K + k + 1] : make_double2(0.0, 0.0);
     const double sc = s_scale[c];
-    __half rh, rl, ih, il;
-    split_f16(v.x * sc, rh, rl);
-    split_f16(v.y * sc, ih, il);
-    const long long off = (long long)(n0 + c) * Kp + k;
-    o[off] = rh;
-    o[plane + off] = rl;
-    o[2 * plane + off] = ih;
-    o[3 * plane + off] = il;
+    __half2 rh, rl, ih, il;
+    split_f16(v0.x * sc, rh.x, rl.x);
+    split_f16(v0.y * sc, ih.x, il.x);
+    split_f16(v1.x * sc, rh.y, rl.y);
+    split_f16(v1.y * sc, ih.y, il.y);
+    __half2* o2 = reinterpret_cast<__half2*>(o + (long long)(n0 + c) * Kp + k);
+    const long long p2 = plane >> 1;
+    o2[0] = rh;
+    o2[p2] = rl;
+    o2[2 * p2] = ih;
+    o2[3 * p2] = il;
   }
 }
 
@@ -586,7 +606,7 @@ static int launch_split_slab(bool a_role, int rows, int K, int Kp, const double2
                              long long st, __half* out, int* ex, int batch, const int* steps,
                              int step, cudaStream_t stream) {
   static int done_a[64], done_b[64];
-  const int smem = R * K * (int)sizeof(double2);
+  const int smem = R * (a_role ? slab_a_stride<R>(K) : K) * (int)sizeof(double2);
   dim3 g((unsigned)((rows + R - 1) / R), batch);
   if (a_role) {
     EUV_CUDA_TRY(ensure_smem(split_a_slab_kernel<R>, smem, done_a));
