@@ -51,6 +51,7 @@ EXPORTS = (
 EUV_KNOB_ABBE_SPLIT = 1
 EUV_KNOB_LU_CLUSTER = 2
 EUV_KNOB_ZGEMM_ROWS = 3
+EUV_KNOB_LU_SUBST_COLS = 4
 EUV_ORDERS_DIAMOND = 0
 EUV_ORDERS_ELLIPSE = 1
 EUV_ORDERS_BOX = 2

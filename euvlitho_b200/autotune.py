@@ -14,6 +14,8 @@ Knobs (``EUV_KNOB_*`` in include/euvl_b200.h):
   resident CTAs);
 * ``lu_cluster``  -- key (n, batch) of an LU: the smallest CTA cluster that
   factors a panel (built in: the fewest CTAs whose registers hold its rows);
+* ``lu_subst_cols`` -- key (n, batch) of an LU solve: right-hand sides per CTA,
+  8 or 12 (built in: 12 where that takes fewer waves of CTAs);
 * ``zgemm_rows``  -- key (m, batch) of the FP64 GEMM: 64- or 32-row tiles
   (FP64 form only; the mixed form's products run on the split-FP16x3 kernel).
 
@@ -31,9 +33,10 @@ import torch
 from . import _lib as L
 
 KNOBS = {"abbe_split": L.EUV_KNOB_ABBE_SPLIT, "lu_cluster": L.EUV_KNOB_LU_CLUSTER,
-         "zgemm_rows": L.EUV_KNOB_ZGEMM_ROWS}
+         "lu_subst_cols": L.EUV_KNOB_LU_SUBST_COLS, "zgemm_rows": L.EUV_KNOB_ZGEMM_ROWS}
 CANDIDATES = {"abbe_split": (1, 2, 3, 4, 6, 8, 12, 16, 24, 32),
               "lu_cluster": (1, 2, 4, 8),
+              "lu_subst_cols": (8, 12),
               "zgemm_rows": (64, 32)}
 
 
@@ -107,7 +110,8 @@ def shapes(batch) -> Dict[str, List[Tuple[int, int]]]:
     """The keys each knob sees in one run of the batch."""
     plan = batch.plan
     N, U = plan.orders.n, batch.U
-    out = {"abbe_split": [(U, batch.ax.shape[1])], "lu_cluster": [(N, U)]}
+    out = {"abbe_split": [(U, batch.ax.shape[1])], "lu_cluster": [(N, U)],
+           "lu_subst_cols": [(N, U)]}
     if plan.precision == L.EUV_PREC_FP64:
         out["zgemm_rows"] = [(N, U)]
     return out

@@ -66,6 +66,7 @@ bool knob_value_ok(int knob, int value) {
     case EUV_KNOB_ABBE_SPLIT: return value >= 1 && value <= 64;
     case EUV_KNOB_LU_CLUSTER: return value == 1 || value == 2 || value == 4 || value == 8;
     case EUV_KNOB_ZGEMM_ROWS: return value == 32 || value == 64;
+    case EUV_KNOB_LU_SUBST_COLS: return value == 8 || value == 12;
     default: return false;
   }
 }

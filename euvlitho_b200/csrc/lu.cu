@@ -526,7 +526,10 @@ int lu_factor(int n, double2* A, long long lda, long long sa, int* ipiv, int* in
 //   off-diagonal   : x(r) -= T(r, block) x(block) for the rows below (forward)
 //                    or above (backward).  RC = 8 runs it on the FP64 tensor
 //                    path: 8-row tiles x 8 right-hand sides x K = 4 DMMAs, four
-//                    per complex step, two tiles' loads in flight per warp.
+//                    per complex step, two tiles' loads in flight per warp;
+//                    RC = 12 (two column tiles, the second half used) when the
+//                    launch then takes fewer waves (24 units x 67 columns: 144
+//                    CTAs instead of 216 on 148 SMs).
 // Replaces 2*ceil(n/32) trsm launches + as many K=32 GEMMs per solve.
 constexpr int LS_THREADS = 512;
 constexpr int LS_WARPS = LS_THREADS / 32;
@@ -563,21 +566,27 @@ static_assert(2 * LS_THREADS == LS_BLK * LS_BLK, "DiagPrefetch covers the block"
 template <int RC>
 __device__ __forceinline__ void update_rows(double2* xs, int n, const double2* LU, long long lda,
                                             int j0, int jb, int r_lo, int r_hi, int tid) {
-  if constexpr (RC == 8) {
+  if constexpr (RC == 8 || RC == 12) {
+    // NT column tiles of 8 right-hand sides (RC = 12: the second tile half
+    // used); each row tile's L fragment serves all of them.  UT row tiles'
+    // loads in flight per warp (one at RC = 12, for the registers).
+    constexpr int NT = (RC + 7) / 8, UT = RC == 8 ? 2 : 1;
     const int lane = tid & 31, warp = tid >> 5, kq = lane & 3, g = lane >> 2;
-    double br[8], bi[8];  // B fragments: x(j0 + 4ks + kq) of right-hand side g
+    double br[NT][8], bi[NT][8];  // B fragments: x(j0 + 4ks + kq) of right-hand side 8nt + g
 #pragma unroll
-    for (int ks = 0; ks < 8; ++ks) {
-      const int q = 4 * ks + kq;
-      const double2 v = q < jb ? xs[g * n + j0 + q] : make_double2(0.0, 0.0);
-      br[ks] = v.x;
-      bi[ks] = v.y;
-    }
+    for (int nt = 0; nt < NT; ++nt)
+#pragma unroll
+      for (int ks = 0; ks < 8; ++ks) {
+        const int q = 4 * ks + kq, c = 8 * nt + g;
+        const double2 v = (q < jb && c < RC) ? xs[c * n + j0 + q] : make_double2(0.0, 0.0);
+        br[nt][ks] = v.x;
+        bi[nt][ks] = v.y;
+      }
     const int ntiles = (r_hi - r_lo + 7) / 8;
-    for (int t = warp; t < ntiles; t += 2 * LS_WARPS) {
-      double2 a[2][8];
+    for (int t = warp; t < ntiles; t += UT * LS_WARPS) {
+      double2 a[UT][8];
 #pragma unroll
-      for (int u = 0; u < 2; ++u) {
+      for (int u = 0; u < UT; ++u) {
         const int tt = t + u * LS_WARPS, r = r_lo + tt * 8 + g;
         const bool rok = tt < ntiles && r < r_hi;
 #pragma unroll
@@ -587,24 +596,28 @@ __device__ __forceinline__ void update_rows(double2* xs, int n, const double2* L
         }
       }
 #pragma unroll
-      for (int u = 0; u < 2; ++u) {
+      for (int u = 0; u < UT; ++u) {
         const int tt = t + u * LS_WARPS;
         if (tt >= ntiles) break;  // warp-uniform
-        double cr0 = 0.0, cr1 = 0.0, ci0 = 0.0, ci1 = 0.0;
-#pragma unroll
-        for (int ks = 0; ks < 8; ++ks) {
-          dmma884(cr0, cr1, a[u][ks].x, br[ks]);
-          dmma884(cr0, cr1, -a[u][ks].y, bi[ks]);
-          dmma884(ci0, ci1, a[u][ks].x, bi[ks]);
-          dmma884(ci0, ci1, a[u][ks].y, br[ks]);
-        }
         const int r = r_lo + tt * 8 + g;
-        if (r < r_hi) {
-          double2* p0 = &xs[(2 * kq) * n + r];
-          double2* p1 = &xs[(2 * kq + 1) * n + r];
-          const double2 o0 = *p0, o1 = *p1;
-          *p0 = make_double2(o0.x - cr0, o0.y - ci0);
-          *p1 = make_double2(o1.x - cr1, o1.y - ci1);
+#pragma unroll
+        for (int nt = 0; nt < NT; ++nt) {
+          double cr0 = 0.0, cr1 = 0.0, ci0 = 0.0, ci1 = 0.0;
+#pragma unroll
+          for (int ks = 0; ks < 8; ++ks) {
+            dmma884(cr0, cr1, a[u][ks].x, br[nt][ks]);
+            dmma884(cr0, cr1, -a[u][ks].y, bi[nt][ks]);
+            dmma884(ci0, ci1, a[u][ks].x, bi[nt][ks]);
+            dmma884(ci0, ci1, a[u][ks].y, br[nt][ks]);
+          }
+          const int c0 = 8 * nt + 2 * kq;
+          if (r < r_hi && c0 < RC) {
+            double2* p0 = &xs[c0 * n + r];
+            double2* p1 = &xs[(c0 + 1) * n + r];
+            const double2 o0 = *p0, o1 = *p1;
+            *p0 = make_double2(o0.x - cr0, o0.y - ci0);
+            *p1 = make_double2(o1.x - cr1, o1.y - ci1);
+          }
         }
       }
     }
@@ -629,11 +642,19 @@ template <int RC>
 __global__ void __launch_bounds__(LS_THREADS) lu_subst_kernel(int n, int nrhs, const double2* LU,
                                                               long long lda, long long sa,
                                                               double2* B, long long ldb,
-                                                              long long sb) {
+                                                              long long sb, const int* order,
+                                                              long long ostride) {
   extern __shared__ double2 xs[];
   __shared__ double2 ds[LS_BLK][LS_BLK + 1];
   const int b = blockIdx.y, c0 = blockIdx.x * RC;
   const int nc = (nrhs - c0) < RC ? (nrhs - c0) : RC;
+  if (order != nullptr) {
+    // every column of this CTA is an empty source slot (order < 0): its
+    // right-hand sides are zero and so is the solution, already in place
+    bool any = false;
+    for (int c = 0; c < nc; ++c) any |= order[(long long)b * ostride + c0 + c] >= 0;
+    if (!any) return;  // the same for every thread of the CTA
+  }
   LU += (long long)b * sa;
   B += (long long)b * sb;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -698,32 +719,55 @@ __global__ void __launch_bounds__(LS_THREADS) lu_subst_kernel(int n, int nrhs, c
 
 template <int RC>
 static int launch_subst(int n, int nrhs, const double2* LU, long long lda, long long sa,
-                        double2* B, long long ldb, long long sb, int batch, cudaStream_t stream) {
+                        double2* B, long long ldb, long long sb, int batch, const int* order,
+                        long long ostride, cudaStream_t stream) {
   static int smem_done[64];
   const int smem = (int)((size_t)RC * n * sizeof(double2));
   EUV_CUDA_TRY(ensure_smem(lu_subst_kernel<RC>, smem, smem_done));
   dim3 grid((nrhs + RC - 1) / RC, batch);
-  lu_subst_kernel<RC><<<grid, LS_THREADS, smem, stream>>>(n, nrhs, LU, lda, sa, B, ldb, sb);
+  lu_subst_kernel<RC><<<grid, LS_THREADS, smem, stream>>>(n, nrhs, LU, lda, sa, B, ldb, sb, order,
+                                                          ostride);
   EUV_LAUNCH_CHECK();
   return EUV_OK;
 }
 
 int lu_solve(int n, int nrhs, const double2* LU, long long lda, long long sa, const int* ipiv,
-             double2* B, long long ldb, long long sb, int batch, cudaStream_t stream) {
+             double2* B, long long ldb, long long sb, int batch, cudaStream_t stream,
+             const int* order, long long ostride) {
   if (n <= 0 || nrhs <= 0 || batch <= 0) return EUV_OK;
   dim3 gs((nrhs + 127) / 128, batch);
   lu_laswp_kernel<<<gs, 128, 0, stream>>>(n, nrhs, 0, n, 0, 0, B, ldb, sb, ipiv, n, 0);
   EUV_LAUNCH_CHECK();
   if (batch <= 65535) {
     const size_t col = (size_t)n * sizeof(double2);
+    // 12 right-hand sides per CTA where that takes fewer waves than 8 (one CTA
+    // per SM either way: the resident columns fill its shared memory), or where
+    // the tuning table says so
+    if (12 * col <= LS_SMEM_MAX && nrhs >= 12) {
+      const int tuned = tune_lookup(EUV_KNOB_LU_SUBST_COLS, n, batch);
+      bool twelve = tuned == 12;
+      if (tuned == 0) {
+        int sms = 0, dev = 0;
+        EUV_CUDA_TRY(cudaGetDevice(&dev));
+        EUV_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        const long long w8 = ((long long)((nrhs + 7) / 8) * batch + sms - 1) / sms;
+        const long long w12 = ((long long)((nrhs + 11) / 12) * batch + sms - 1) / sms;
+        // with empty source slots skipped the launch holds fewer live CTAs than
+        // its grid, so a tie in waves goes to 12 (measured: 24 units of N = 961,
+        // 96 slots for families of 96, 92 and 12 sources, step 25.35 -> 24.97 ms)
+        twelve = sms > 0 && (w12 < w8 || (order != nullptr && w12 == w8));
+      }
+      if (twelve)
+        return launch_subst<12>(n, nrhs, LU, lda, sa, B, ldb, sb, batch, order, ostride, stream);
+    }
     if (8 * col <= LS_SMEM_MAX && nrhs >= 8)
-      return launch_subst<8>(n, nrhs, LU, lda, sa, B, ldb, sb, batch, stream);
+      return launch_subst<8>(n, nrhs, LU, lda, sa, B, ldb, sb, batch, order, ostride, stream);
     if (4 * col <= LS_SMEM_MAX && nrhs >= 4)
-      return launch_subst<4>(n, nrhs, LU, lda, sa, B, ldb, sb, batch, stream);
+      return launch_subst<4>(n, nrhs, LU, lda, sa, B, ldb, sb, batch, order, ostride, stream);
     if (2 * col <= LS_SMEM_MAX && nrhs >= 2)
-      return launch_subst<2>(n, nrhs, LU, lda, sa, B, ldb, sb, batch, stream);
+      return launch_subst<2>(n, nrhs, LU, lda, sa, B, ldb, sb, batch, order, ostride, stream);
     if (col <= LS_SMEM_MAX)
-      return launch_subst<1>(n, nrhs, LU, lda, sa, B, ldb, sb, batch, stream);
+      return launch_subst<1>(n, nrhs, LU, lda, sa, B, ldb, sb, batch, order, ostride, stream);
   }
   // n too large for one column of X in shared memory: blocked trsm + GEMM
   // forward: L y = b (unit lower)
@@ -783,5 +827,5 @@ extern "C" int euv_lu_solve(int n, int nrhs, const euv_c64* d_lu, int lda, long 
   }
   return euv::lu_solve(n, nrhs, reinterpret_cast<const double2*>(d_lu), lda, stride_a, d_ipiv,
                        reinterpret_cast<double2*>(d_b), ldb, stride_b, batch,
-                       (cudaStream_t)stream);
+                       (cudaStream_t)stream, nullptr, 0);
 }

@@ -32,8 +32,11 @@ int zgemm(int m, int n, int k, cplx alpha, const double* scale, const double2* a
           cudaStream_t stream);
 int lu_factor(int n, double2* A, long long lda, long long sa, int* ipiv, int* info, int batch,
               cudaStream_t stream);
+// order (optional): per batch entry, ostride ints whose first nrhs mark the
+// right-hand sides; a CTA whose columns are all < 0 (zero columns) is skipped
 int lu_solve(int n, int nrhs, const double2* LU, long long lda, long long sa, const int* ipiv,
-             double2* B, long long ldb, long long sb, int batch, cudaStream_t stream);
+             double2* B, long long ldb, long long sb, int batch, cudaStream_t stream,
+             const int* order = nullptr, long long ostride = 0);
 int gemm_mixed(int m, int n, int k, cplx alpha, const double* scale, const double2* a,
                long long lda, long long sa, const double2* b, long long ldb, long long sb,
                cplx beta, double2* c, long long ldc, long long sc, cplx diag, int batch,
@@ -1026,7 +1029,10 @@ extern "C" int euv_amp(const euv_amp_desc* d, const euv_c64* d_spectra, euv_c64*
     dim3 gs(grid1((long long)N * ns, bs), U);
     src_rhs_kernel<<<gs, bs, 0, stream>>>(N, ns, d->d_src_order, d->d_src_2kz, w.E);
     EUV_LAUNCH_CHECK();
-    if ((rc = lu_solve(N, ns, w.G, N, nn, w.ipiv, w.E, N, (long long)N * ns, U, stream))) return rc;
+    // empty source slots (order < 0, zero columns of E) skip their CTAs
+    if ((rc = lu_solve(N, ns, w.G, N, nn, w.ipiv, w.E, N, (long long)N * ns, U, stream,
+                       d->d_src_order, ns)))
+      return rc;
     // Y Z for the source columns: a product, so the mixed form takes it on the
     // tensor cores (split-FP16x3, ~1e-6 relative) like the matrix functions; the
     // solve above stays FP64

@@ -539,6 +539,9 @@ int euv_zgemm_mixed(int m, int n, int k, euv_c64 alpha, const double* d_scale,
 #define EUV_KNOB_LU_CLUSTER 2 /* key (n, batch) of the LU: smallest CTA cluster of a panel,
                                  1, 2, 4 or 8 (built in: the fewest CTAs that hold the rows) */
 #define EUV_KNOB_ZGEMM_ROWS 3 /* key (m, batch) of the FP64 GEMM: row tile 64 or 32 */
+#define EUV_KNOB_LU_SUBST_COLS 4 /* key (n, batch) of an LU solve: right-hand sides per CTA,
+                                    8 or 12 (built in: 12 where that takes fewer waves,
+                                    or as many when empty source slots are skipped) */
 int euv_tune_set(int knob, int k0, int k1, int value);
 int euv_tune_get(int knob, int k0, int k1);
 void euv_tune_clear(void);

@@ -34,7 +34,8 @@ def test_tune_table_set_get_clear(lib):
 
 
 @pytest.mark.parametrize("knob,value", [(L.EUV_KNOB_LU_CLUSTER, 3), (L.EUV_KNOB_ABBE_SPLIT, 65),
-                                        (L.EUV_KNOB_ZGEMM_ROWS, 48), (99, 1)])
+                                        (L.EUV_KNOB_ZGEMM_ROWS, 48), (L.EUV_KNOB_LU_SUBST_COLS, 16),
+                                        (99, 1)])
 def test_tune_table_rejects_values_a_kernel_cannot_take(lib, knob, value):
     assert lib.euv_tune_set(knob, 1, 1, value) == L.EUV_ERR_BAD_ARG
     assert lib.euv_tune_get(knob, 1, 1) == 0

@@ -71,7 +71,10 @@ def test_zgemm_step_copy(cuda):
 
 
 @pytest.mark.parametrize("n,nrhs,batch", [(1, 1, 1), (31, 5, 2), (121, 121, 4), (200, 17, 2), (300, 9, 3),
-                                           (961, 40, 2), (1300, 8, 1), (1681, 16, 1)])
+                                           (961, 40, 2), (1300, 8, 1), (1681, 16, 1),
+                                           # 12 right-hand sides per CTA (fewer waves than 8):
+                                           # the bench shape, and ragged last groups
+                                           (961, 67, 24), (200, 20, 100), (150, 25, 130)])
 def test_lu_solve(cuda, n, nrhs, batch):
     import torch
     rng = np.random.default_rng(n)
