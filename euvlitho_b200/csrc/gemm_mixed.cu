@@ -449,7 +449,18 @@ __global__ void split_b_kernel(int K, int N, int Kp, const double2* B, long long
 constexpr size_t MX_SLAB_BYTES = 100 * 1024;      // several CTAs per SM
 constexpr size_t MX_SLAB_BYTES_ONE = 200 * 1024;  // one row or column per CTA
 constexpr int MX_SLAB_THREADS = 256;
-constexpr int MX_SLAB_UNROLL = 8;
+// 16-byte asynchronous copy global -> shared (zero-filled when !pred): the
+// whole slab of a CTA is in flight at once, not eight loads per thread
+__device__ __forceinline__ void slab_cp16(void* smem, const void* gmem, bool pred) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gmem),
+               "r"(pred ? 16 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void slab_cp_wait() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
 
 // Row stride (elements) of the A slab: K rounded up to 8, plus 8 / R, so that
 // the loads' stores (R consecutive rows per run of lanes) and the row-wise
@@ -472,21 +483,13 @@ __global__ void __launch_bounds__(MX_SLAB_THREADS)
   const int rows = M - m0 < R ? M - m0 : R;
   A += (long long)b * sa;
   // consecutive threads take consecutive rows of a column (runs of R * 16
-  // bytes); eight loads in flight per thread before their stores
-  for (int base = 0; base < K * R; base += MX_SLAB_THREADS * MX_SLAB_UNROLL) {
-    double2 v[MX_SLAB_UNROLL];
-#pragma unroll
-    for (int u = 0; u < MX_SLAB_UNROLL; ++u) {
-      const int t = base + threadIdx.x + u * MX_SLAB_THREADS;
-      const int k = t / R, r = t % R;
-      v[u] = (t < K * R && r < rows) ? A[(m0 + r) + (long long)k * lda] : make_double2(0.0, 0.0);
-    }
-#pragma unroll
-    for (int u = 0; u < MX_SLAB_UNROLL; ++u) {
-      const int t = base + threadIdx.x + u * MX_SLAB_THREADS;
-      if (t < K * R) slab[(t % R) * Ks + t / R] = v[u];
-    }
+  // bytes); every copy of the slab in flight before the first wait
+  for (int t = threadIdx.x; t < K * R; t += MX_SLAB_THREADS) {
+    const int k = t / R, r = t % R;
+    const bool ok = r < rows;
+    slab_cp16(&slab[r * Ks + k], ok ? A + (m0 + r) + (long long)k * lda : A, ok);
   }
+  slab_cp_wait();
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (warp < R) {
@@ -538,20 +541,12 @@ __global__ void __launch_bounds__(MX_SLAB_THREADS)
   const int n0 = blockIdx.x * R;
   const int cols = N - n0 < R ? N - n0 : R;
   B += (long long)b * sb;
-  for (int base = 0; base < K * R; base += MX_SLAB_THREADS * MX_SLAB_UNROLL) {
-    double2 v[MX_SLAB_UNROLL];
-#pragma unroll
-    for (int u = 0; u < MX_SLAB_UNROLL; ++u) {
-      const int t = base + threadIdx.x + u * MX_SLAB_THREADS;
-      const int c = t / K, k = t % K;
-      v[u] = (t < K * R && c < cols) ? B[k + (long long)(n0 + c) * ldb] : make_double2(0.0, 0.0);
-    }
-#pragma unroll
-    for (int u = 0; u < MX_SLAB_UNROLL; ++u) {
-      const int t = base + threadIdx.x + u * MX_SLAB_THREADS;
-      if (t < K * R) slab[t] = v[u];
-    }
+  for (int t = threadIdx.x; t < K * R; t += MX_SLAB_THREADS) {
+    const int c = t / K, k = t % K;
+    const bool ok = c < cols;
+    slab_cp16(&slab[t], ok ? B + k + (long long)(n0 + c) * ldb : B, ok);
   }
+  slab_cp_wait();
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (warp < R) {

@@ -214,11 +214,12 @@ __global__ void build_dg_kernel(SliceParams p, const double2* spectra, const int
                                 const int* lidx, const int* midx, const double* kx0,
                                 const double* ky0, const int* polar, double2* D, double2* G,
                                 int want_d, int want_g) {
-  const int u = blockIdx.y;
+  // grid: x = column j, y = row chunk, z = unit (no 64-bit division per element)
+  const int u = blockIdx.z, j = blockIdx.x;
+  const int i = blockIdx.y * blockDim.x + threadIdx.x;
+  if (i >= p.n) return;
   const long long nn = (long long)p.n * p.n;
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= nn) return;
-  const int i = (int)(t % p.n), j = (int)(t / p.n);
+  const long long t = (long long)j * p.n + i;
   const int li = lidx[i], mi = midx[i], lj = lidx[j], mj = midx[j];
   const int l = li - lj + 2 * p.lmax, m = mi - mj + 2 * p.mmax;
   const double2* sp = spectra + ((long long)spec_of_unit[u] * p.n_slices + p.slice) * p.lr2 * p.mr2;
@@ -820,6 +821,7 @@ extern "C" int euv_amp(const euv_amp_desc* d, const euv_c64* d_spectra, euv_c64*
   const long long nn = (long long)N * N;
   const int bs = 256;
   const dim3 ge(grid1(nn, bs), U);
+  const dim3 gdg((unsigned)N, (unsigned)((N + bs - 1) / bs), U);  // build_dg: column, rows, unit
   const cplx one = mk(1.0, 0.0), zero = mk(0.0, 0.0), mi = mk(0.0, -1.0);
   int m_max = d->m_max > 0 ? d->m_max : derive_m_max(d);
   if (m_max > kMaxSteps) m_max = kMaxSteps;
@@ -926,7 +928,7 @@ extern "C" int euv_amp(const euv_amp_desc* d, const euv_c64* d_spectra, euv_c64*
     const bool bottom = (n == NS - 1);
     const bool need_g = bottom || d->refresh_sigma;
     // bottom slice sigma is used for every slice unless refresh_sigma (header.h:1327-1353)
-    build_dg_kernel<<<ge, bs, 0, stream>>>(q, spec, d->d_spec, d->d_lindex, d->d_mindex, d->d_kx0,
+    build_dg_kernel<<<gdg, bs, 0, stream>>>(q, spec, d->d_spec, d->d_lindex, d->d_mindex, d->d_kx0,
                                            d->d_ky0, d->d_polar, w.D, w.G, 1,
                                            need_g ? (euler_f > 0 ? 2 : 1) : 0);
     EUV_LAUNCH_CHECK();
@@ -950,7 +952,7 @@ extern "C" int euv_amp(const euv_amp_desc* d, const euv_c64* d_spectra, euv_c64*
     } else if (d->refresh_sigma && euler_f > 0) {
       // Z = (I - E_n)^-1 (I - E_{n+1}) X  (= G_n^-1 G_{n+1} X)
       SliceParams qp = slice_params(n + 1);
-      build_dg_kernel<<<ge, bs, 0, stream>>>(qp, spec, d->d_spec, d->d_lindex, d->d_mindex,
+      build_dg_kernel<<<gdg, bs, 0, stream>>>(qp, spec, d->d_spec, d->d_lindex, d->d_mindex,
                                              d->d_kx0, d->d_ky0, d->d_polar, nullptr, w.Gp, 0, 2);
       EUV_LAUNCH_CHECK();
       if ((rc = gemm(N, N, N, mk(-1.0, 0.0), nullptr, w.Gp, N, nn, X, N, nn, one, w.Z, N, nn, zero,
@@ -963,7 +965,7 @@ extern "C" int euv_amp(const euv_amp_desc* d, const euv_c64* d_spectra, euv_c64*
     } else if (d->refresh_sigma) {
       // Z = G_n^-1 G_{n+1} X
       SliceParams qp = slice_params(n + 1);
-      build_dg_kernel<<<ge, bs, 0, stream>>>(qp, spec, d->d_spec, d->d_lindex, d->d_mindex,
+      build_dg_kernel<<<gdg, bs, 0, stream>>>(qp, spec, d->d_spec, d->d_lindex, d->d_mindex,
                                              d->d_kx0, d->d_ky0, d->d_polar, nullptr, w.Gp, 0, 1);
       EUV_LAUNCH_CHECK();
       if ((rc = gemm(N, N, N, one, nullptr, w.Gp, N, nn, X, N, nn, zero, w.Z, N, nn, zero, U))) return rc;
