@@ -216,6 +216,21 @@ __global__ void build_dg_kernel(SliceParams p, const double2* spectra, const int
                                 int want_d, int want_g) {
   // grid: x = column j, y = row chunk, z = unit (no 64-bit division per element)
   const int u = blockIdx.z, j = blockIdx.x;
+  // the unit's and column's constants once per CTA: no FP64 division per element
+  __shared__ double s_c[8];  // 2pi/dx, 2pi/dy, 1/k, kx_j, ky_j, kx0, ky0
+  if (threadIdx.x == 0) {
+    const double twopi = 6.283185307179586476925286766559;
+    const double dxu = p.dxs ? p.dxs[u] : p.dx, dyu = p.dys ? p.dys[u] : p.dy;
+    const double gx = twopi / dxu, gy = twopi / dyu;
+    s_c[0] = gx;
+    s_c[1] = gy;
+    s_c[2] = 1.0 / p.k;
+    s_c[3] = kx0[u] + gx * lidx[j];
+    s_c[4] = ky0[u] + gy * midx[j];
+    s_c[5] = kx0[u];
+    s_c[6] = ky0[u];
+  }
+  __syncthreads();
   const int i = blockIdx.y * blockDim.x + threadIdx.x;
   if (i >= p.n) return;
   const long long nn = (long long)p.n * p.n;
@@ -226,10 +241,9 @@ __global__ void build_dg_kernel(SliceParams p, const double2* spectra, const int
   const double2 f2 = sp[l + (long long)p.lr2 * m];
   const cplx F = mk(f2.x, f2.y);
   const bool dc = (l == 2 * p.lmax) && (m == 2 * p.mmax);
-  const double twopi = 6.283185307179586476925286766559;
-  const double dxu = p.dxs ? p.dxs[u] : p.dx, dyu = p.dys ? p.dys[u] : p.dy;
-  const double kxi = kx0[u] + twopi * li / dxu, kyi = ky0[u] + twopi * mi / dyu;
-  const double kxj = kx0[u] + twopi * lj / dxu, kyj = ky0[u] + twopi * mj / dyu;
+  const double gx = s_c[0], gy = s_c[1], ik = s_c[2];
+  const double kxi = s_c[5] + gx * li, kyi = s_c[6] + gy * mi;
+  const double kxj = s_c[3], kyj = s_c[4];
   const int pol = polar[u];
   if (want_d) {
     cplx eps = p.eps_m1 * F;
@@ -238,9 +252,9 @@ __global__ void build_dg_kernel(SliceParams p, const double2* spectra, const int
     cplx v = (p.k * p.k) * eps;
     if (pol == 0) {
       // -i * eta * kx_j, eta = i 2 pi l / dx * leps  ->  +2 pi l/dx * leps * kx_j
-      v = v + (twopi * (double)(l - 2 * p.lmax) / dxu * kxj) * leps;
+      v = v + (gx * (double)(l - 2 * p.lmax) * kxj) * leps;
     } else {
-      v = v + (twopi * (double)(m - 2 * p.mmax) / dyu * kyj) * leps;
+      v = v + (gy * (double)(m - 2 * p.mmax) * kyj) * leps;
     }
     if (i == j) v.x -= kxi * kxi + kyi * kyi;
     D[(long long)u * nn + t] = make_double2(v.x, v.y);
@@ -251,11 +265,11 @@ __global__ void build_dg_kernel(SliceParams p, const double2* spectra, const int
     const double kpi = pol == 0 ? kxi : kyi, kpj = pol == 0 ? kxj : kyj;
     if (want_g == 2) {
       // E = diag(kp/k) sigma diag(kp/k), with G = i k (I - E)
-      cplx v = (kpi / p.k * (kpj / p.k)) * sig;
+      cplx v = (kpi * ik * (kpj * ik)) * sig;
       G[(long long)u * nn + t] = make_double2(v.x, v.y);
     } else {
       // G = i (k delta - kp_i/k sig kp_j)
-      cplx a = (-kpi / p.k * kpj) * sig;
+      cplx a = (-kpi * ik * kpj) * sig;
       if (i == j) a.x += p.k;
       cplx v = cmul_i(a);
       G[(long long)u * nn + t] = make_double2(v.x, v.y);
