@@ -571,7 +571,7 @@ __global__ void flag_singular_kernel(const int* info, int n, int* status) {
 // GEMM dispatch by precision (FP64 DMMA, or split-FP16x3 tcgen05 tensor cores for
 // the bulk products of the mixed form; `status` receives EUV_STATUS_TIMEOUT).
 // Gemm reuse flags (mixed form only): the previous call through the same Gemm
-// split this unchanged operand in the same role and shape, so its TF32 planes
+// split this unchanged operand in the same role and shape, so its fp16 planes
 // in the workspace are current.
 constexpr int kReuseA = 1;
 constexpr int kReuseB = 2;

@@ -1,9 +1,9 @@
 // Blackwell (sm_100a) tensor-core plumbing shared by the tcgen05 kernels (the
 // mixed-precision complex GEMM, the CNN's convolutions and dense layers):
 // mbarriers with bounded waits, TMA tensor loads, UMMA shared-memory
-// descriptors for 64-byte-swizzled K-major tiles, tcgen05.mma of kind tf32,
-// TMEM loads, the FP64/FP32 -> (hi, lo) TF32 split and the driver's
-// tensor-map encoder.
+// descriptors for 64-byte-swizzled K-major tiles, tcgen05.mma of kind tf32
+// (the CNN; the mixed GEMM issues kind::f16 itself), TMEM loads, the
+// FP64/FP32 -> (hi, lo) TF32 split and the driver's tensor-map encoder.
 #pragma once
 #include <cuda.h>
 #include "common.cuh"
