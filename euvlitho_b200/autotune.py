@@ -84,7 +84,9 @@ def save(picks: Dict[Tuple[str, int, int], int], path: Optional[str] = None, dev
     for (name, k0, k1), v in picks.items():
         mine["%s/%d/%d" % (name, k0, k1)] = int(v)
     os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
-    tmp = path + ".tmp"
+    # one temporary file per process: ranks tuning at once (one process per GPU)
+    # each replace the cache atomically; the last writer's picks stay
+    tmp = "%s.tmp.%d" % (path, os.getpid())
     with open(tmp, "w") as f:
         json.dump(data, f, indent=1, sort_keys=True)
     os.replace(tmp, path)

@@ -1,6 +1,7 @@
 """The tuning table of the C ABI and the autotuner's cache file (CPU: no
 launch; the GPU side runs in bench.py and test_gpu_autotune)."""
 import json
+import os
 
 import pytest
 
@@ -54,3 +55,26 @@ def test_cache_round_trip(lib, tmp_path, monkeypatch):
     monkeypatch.setattr(A, "gpu_name", lambda device=None: "another GPU")
     lib.euv_tune_clear()
     assert A.load(path) == 0          # picks are per GPU model
+
+
+def _save_many(args):
+    path, rank = args
+    from euvlitho_b200 import autotune as A2
+    A2.gpu_name = lambda device=None: "NVIDIA B200"  # no GPU needed to write the cache
+    for i in range(200):
+        A2.save({("abbe_split", 24, 100 + rank): 1 + (i % 4)}, path)
+    return rank
+
+
+def test_cache_save_from_concurrent_ranks(tmp_path):
+    """One process per GPU may tune and save at once (torchrun): every save
+    replaces the cache atomically through its own temporary file, so no rank
+    fails and the file stays valid JSON."""
+    import multiprocessing as mp
+    path = str(tmp_path / "tuning.json")
+    with mp.get_context("spawn").Pool(4) as pool:
+        assert sorted(pool.map(_save_many, [(path, r) for r in range(4)])) == [0, 1, 2, 3]
+    with open(path) as f:
+        data = json.load(f)
+    assert len(data) == 1 and all(v in (1, 2, 3, 4) for v in next(iter(data.values())).values())
+    assert not [p for p in os.listdir(str(tmp_path)) if ".tmp" in p]
