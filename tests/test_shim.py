@@ -114,3 +114,14 @@ def test_cpp_ampS_shim_matches_oracle(cuda, tmp_path):
     got = np.fromfile(tmp_path / "ax.bin", np.complex128).reshape(len(srcs), len(li))
     for s, key in enumerate(srcs):
         assert rel_err(got[s], ref[key]) < 1e-8, key
+
+
+def test_integration_doc_shows_the_compiled_shim_verbatim():
+    """INTEGRATION.md prints the binding a maintainer adds to the reference;
+    the files compiled above must be exactly those listings."""
+    import re
+    doc = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    blocks = [b.strip() for b in re.findall(r"```(?:cpp|c\+\+|c)\n(.*?)```", doc, re.S)]
+    for name in ("ampS_shim.h", "ampS_shim.cpp"):
+        with open(os.path.join(SHIM, name)) as f:
+            assert f.read().strip() in blocks, name
